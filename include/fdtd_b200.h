@@ -1,0 +1,187 @@
+/*
+ * fdtd_b200.h — C ABI of the B200 FDTD engine (libfdtd_b200.so).
+ *
+ * Plain C: raw device pointers, sizes and scalars; no C++ or torch types.
+ * Every entry point returns an FDTD_* status; FDTD_OK == 0.  The message for the
+ * last failure on the calling host thread is returned by fdtd_last_error().
+ * Launches are asynchronous on the given cudaStream_t (passed as void*, NULL =
+ * legacy default stream); nothing here synchronises the device except where a
+ * function documents that it returns a host value.
+ *
+ * Memory layout (all fields, coefficients and ψ stripes): C order, k fastest,
+ * idx = (i*Ny + j)*Nz + k, element type double when dtype == FDTD_F64 and float
+ * otherwise — the layout of the reference's cl.Buffer objects
+ * (opencl_fdtd_solver/engine.py:166-187, yee_update.cl:28).  ψ stripes use the
+ * reference face layout (engine.py:290-318): x-normal (2·npml, Ny, Nz),
+ * y-normal (Nx, 2·npml, Nz), z-normal (Nx, Ny, 2·npml); low-face layers first.
+ *
+ * Each declaration names the reference interface it replaces (file:line in the
+ * reference project).
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define FDTD_OK 0
+#define FDTD_ERR_INVALID 1      /* bad argument: shape, pointer, index, size   */
+#define FDTD_ERR_CUDA 2         /* a CUDA runtime call or launch failed        */
+#define FDTD_ERR_DEVICE 3       /* a device-side check failed (see flags)      */
+#define FDTD_ERR_UNSUPPORTED 4  /* valid request this build/device cannot run  */
+
+#define FDTD_F32 0
+#define FDTD_F64 1
+
+#define FDTD_MAX_SOURCES 8      /* pending injections applied by one E launch  */
+#define FDTD_MAX_PLANES 4       /* plane DFT monitors fused into one E launch  */
+#define FDTD_MAX_FREQS 64       /* frequencies per DFT monitor                 */
+
+/* Grid and time-step scalars.  dtm = dt/mu0, dtm_dl = dt/(mu0*dl),
+ * inv_dl = 1/dl, each rounded once to the field dtype by the kernels, as the
+ * reference host does (engine.py:541-544, 634). */
+typedef struct {
+    int32_t nx, ny, nz, npml;
+    int32_t dtype;          /* FDTD_F32 or FDTD_F64                            */
+    int32_t lossy;          /* nonzero: E = ca*E + ...; zero: ca == 1, not read */
+    double dtm, dtm_dl, inv_dl;
+} fdtd_grid;
+
+/* Field state.  E/H hold the state at step n (E^n, H^{n-1/2}).
+ * E_next/H_next receive the fused step's result and must not alias E/H
+ * (the split half-steps update E/H in place and ignore them). */
+typedef struct {
+    void *E[3];
+    void *H[3];
+    void *E_next[3];
+    void *H_next[3];
+    const void *ce[3];      /* dt/(eps0 eps_edge), or cb when lossy            */
+    const void *ca[3];      /* read only when grid.lossy != 0                  */
+} fdtd_fields;
+
+/* CPML: 1-D b, c and 1/(kappa*dl) for the H (offset 1/2) and E (offset 0)
+ * staggers (cpml.py:111-134, engine.py:264-283), and the 12 ψ stripes.
+ * psi_h order: Hx_y, Hx_z, Hy_x, Hy_z, Hz_x, Hz_y;
+ * psi_e order: Ex_y, Ex_z, Ey_x, Ey_z, Ez_x, Ez_y (yee_update.cl:56-58,176-178).
+ * psi_h_next receives the fused step's ψ_H (must not alias psi_h). */
+typedef struct {
+    const void *b_h[3], *c_h[3], *ik_h[3];
+    const void *b_e[3], *c_e[3], *ik_e[3];
+    void *psi_h[6];
+    void *psi_h_next[6];
+    void *psi_e[6];
+} fdtd_cpml;
+
+#define FDTD_SRC_JX 0   /* Ex += -ce_x * amp * w   (sources.cl:26-49)           */
+#define FDTD_SRC_EX 1   /* Ex += amp               (sources.cl:7-21)            */
+
+/* One sheet injection on the constant-z plane z, half-open [i0,i1) x [j0,j1).
+ * amp is the host-side amplitude after the rim renormalisation of
+ * engine.py:512-520; kernels round it to the field dtype. */
+typedef struct {
+    int32_t kind, z, i0, i1, j0, j1, rim_taper, pad_;
+    double amp, rim_edge;
+} fdtd_source;
+
+/* A single-plane DFT accumulated in the E epilogue (no reference class; phase
+ * convention of monitors.py:571-584).  acc: complex128 (re, im pairs),
+ * [ncomp][nfreq][plane cells], components in Ex..Hz bit order of comp_mask,
+ * plane cells in C order of the two remaining axes.  phase: device pointer to
+ * this step's [nfreq][4] doubles (E re, E im, H re, H im). */
+typedef struct {
+    int32_t axis, index, comp_mask, nfreq;
+    double *acc;
+    const double *phase;
+} fdtd_plane_dft;
+
+/* ---- Yee time step ------------------------------------------------------- */
+
+/* H half step, in place: H -= dt/mu0 * curl E with CPML (H^{n-1/2} -> H^{n+1/2}).
+ * Replaces update_H_interior + update_H_pml (yee_update.cl:11-118) as launched
+ * by OpenCLFDTD._update_H (engine.py:540-629). */
+int fdtd_update_H(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
+                  void *stream);
+
+/* E half step, in place, with pending sheet injections applied to E^n before
+ * the update (E = ca*(E + s) + ce*curl H) and plane DFTs of E^{n+1}/H^{n+1/2}.
+ * Replaces update_E_interior + update_E_pml (yee_update.cl:120-238) launched
+ * by OpenCLFDTD._update_E (engine.py:631-722), preceded by the add_source_*
+ * launches made from source callbacks (engine.py:448-538, sources.cl). */
+int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
+                  const fdtd_source *src, int32_t nsrc,
+                  const fdtd_plane_dft *planes, int32_t nplanes, void *stream);
+
+/* One full leapfrog step H -> sources -> E in a single pass over HBM:
+ * reads E/H/psi_h, writes E_next/H_next/psi_h_next (psi_e in place).
+ * Replaces the whole of OpenCLFDTD.step() up to the monitors
+ * (engine.py:724-735): _update_H, the source callbacks' injections, _update_E. */
+int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
+              const fdtd_source *src, int32_t nsrc,
+              const fdtd_plane_dft *planes, int32_t nplanes, void *stream);
+
+/* Immediate sheet injection into Ex (used when a source callback reads fields
+ * after injecting).  Replaces add_source_Jx / add_source_Ex
+ * (sources.cl:7-49, engine.py:448-538). */
+int fdtd_add_source(const fdtd_grid *g, void *Ex, const void *ce_x,
+                    const fdtd_source *src, void *stream);
+
+/* ---- Huygens-box DFT and far field -------------------------------------- */
+
+/* Box (inclusive indices) and packed face layout x0,x1,y0,y1,z0,z1
+ * (monitors.py:396-412). */
+typedef struct {
+    int32_t ix0, ix1, iy0, iy1, iz0, iz1;
+    int32_t off[6];
+    int32_t n_face;
+    int32_t nfreq;
+} fdtd_box;
+
+/* Co-located tangential face DFT at nfreq frequencies, complex128 accumulators
+ * acc[6][nfreq][n_face] (Ex..Hz), phase [nfreq][4] for this step.
+ * Replaces accumulate_dft_faces_fused (dft_farfield.cl:116-230) launched by
+ * OpenCLNear2FarMonitor.__call__ (monitors.py:571-624). */
+int fdtd_dft_faces(const fdtd_grid *g, const void *const E[3], const void *const H[3],
+                   const fdtd_box *box, double *acc, const double *phase, void *stream);
+
+/* Relative change sqrt(sum|cur-prev|^2 / sum|cur|^2) of one frequency slice
+ * over the six face DFTs; writes two doubles (num, den) to out2 (device).
+ * scratch: device doubles, at least 2*fdtd_rel_change_blocks(n) of them.
+ * Replaces dft_rel_change_partial (dft_farfield.cl:237-290) and the host sum
+ * of monitors.py:505-569. */
+int fdtd_rel_change_blocks(int32_t n_face);
+int fdtd_dft_rel_change(const double *cur, const double *prev, int32_t n_face,
+                        int32_t nfreq, int32_t fi, double *scratch, double *out2,
+                        void *stream);
+
+/* Far-field E, H at n_obs points (float64 xyz) from face DFT slice fi:
+ * eh[n_obs][6] complex128 = (Ex,Ey,Ez,Hx,Hy,Hz); nl_scratch: n_obs*6 complex128.
+ * Direct surface sum in float64 with the kernel's sign (eta N_t - r x L).
+ * Replaces farfield_accumulate_nl + farfield_nl_to_eh (dft_farfield.cl:372-635)
+ * launched by OpenCLNear2FarMonitor.get_farfields (monitors.py:644-731). */
+int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl,
+                  double k_wave, double eta0, const double *obs_xyz, int32_t n_obs,
+                  double *nl_scratch, double *eh, void *stream);
+
+/* ---- diagnostics --------------------------------------------------------- */
+
+/* Message for the last non-OK status returned on this host thread. */
+const char *fdtd_last_error(void);
+
+/* Device-side error flags raised by kernels since the last reset (bit 0: a
+ * bounded wait in the fused step timed out).  Synchronises with the device to
+ * read the flag; clears it when reset != 0.  No reference counterpart (the
+ * reference kernels have no device-side waits). */
+int fdtd_device_status(int32_t *flags, int32_t reset);
+
+/* Library build tag, e.g. "fdtd_b200 sm_100a". */
+const char *fdtd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDTD_B200_H */

@@ -1,3 +1,38 @@
-"""B200-native FDTD engine: a drop-in CUDA backend for the OpenCLFDTD API."""
+"""B200-native FDTD engine: a CUDA drop-in for the ``OpenCLFDTD`` API.
+
+Public surface (mirrors the reference ``opencl_fdtd_solver/__init__.py:10-21``,
+with ``CUDAFDTD`` / ``CUDANear2FarMonitor`` in place of the OpenCL classes):
+
+* constants ``C0, MU0, EPS0, ETA0``
+* ``CUDAFDTD`` — Yee/CPML engine on one CUDA device
+* ``CUDANear2FarMonitor`` — Huygens-box DFT + far field
+* ``CUDAPlaneDFTMonitor`` — single-plane DFT fused into the E update
+* ``StepCallback``, ``SourceMonitorMixin``, ``BACKENDS``, ``get_backend``
+* ``near2far_contract`` — tensor-core near-to-far contraction
+* ``EpsilonObjective`` — adjoint ε-gradient behind ``torch.autograd.Function``
+
+Importing the package does not touch CUDA; constructing an engine does.
+"""
 
 __version__ = "0.1.0"
+
+from .constants import C0, EPS0, ETA0, MU0
+from .engine import CUDAFDTD
+from .monitors import CUDANear2FarMonitor, CUDAPlaneDFTMonitor
+from .plugin import BACKENDS, SourceMonitorMixin, StepCallback, get_backend, register_backend
+
+__all__ = [
+    "C0",
+    "MU0",
+    "EPS0",
+    "ETA0",
+    "CUDAFDTD",
+    "CUDANear2FarMonitor",
+    "CUDAPlaneDFTMonitor",
+    "StepCallback",
+    "SourceMonitorMixin",
+    "BACKENDS",
+    "get_backend",
+    "register_backend",
+    "__version__",
+]

@@ -1,0 +1,322 @@
+// extern "C" entry points of libfdtd_b200.so (declared in include/fdtd_b200.h):
+// argument validation, dtype dispatch, status codes and error messages.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/fdtd_b200.h"
+#include "yee_launch.cuh"
+
+namespace fdtd {
+template <typename T>
+cudaError_t launch_dft_faces(int nx, int ny, int nz, const T *const E[3], const T *const H[3],
+                             const fdtd_box &b, double *acc, const double *phase,
+                             cudaStream_t st);
+int rel_change_blocks(int n);
+cudaError_t launch_rel_change(const double *cur, const double *prev, int n, int nfreq, int fi,
+                              double *scratch, double *out2, cudaStream_t st);
+cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double dl,
+                            double k_wave, double eta0, const double *obs, int n_obs,
+                            double *nl, double *eh, cudaStream_t st);
+int read_fused_error(int reset);
+}  // namespace fdtd
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return FDTD_OK;
+    if (e == cudaErrorNotSupported)
+        return fail(FDTD_ERR_UNSUPPORTED, "%s: not supported for this shape/alignment", what);
+    return fail(FDTD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int check_grid(const fdtd_grid *g) {
+    if (!g) return fail(FDTD_ERR_INVALID, "grid is NULL");
+    if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0)
+        return fail(FDTD_ERR_INVALID, "grid shape must be positive, got (%d, %d, %d)", g->nx,
+                    g->ny, g->nz);
+    if (g->ny > 65535 * 8 || g->nx > 65535)
+        return fail(FDTD_ERR_INVALID, "grid too large for the launch geometry (%d, %d, %d)",
+                    g->nx, g->ny, g->nz);
+    if (g->npml < 0) return fail(FDTD_ERR_INVALID, "npml must be >= 0, got %d", g->npml);
+    if (g->dtype != FDTD_F32 && g->dtype != FDTD_F64)
+        return fail(FDTD_ERR_INVALID, "dtype must be FDTD_F32 or FDTD_F64, got %d", g->dtype);
+    return FDTD_OK;
+}
+
+int check_fields(const fdtd_grid *g, const fdtd_fields *f, bool need_next) {
+    if (!f) return fail(FDTD_ERR_INVALID, "fields is NULL");
+    for (int c = 0; c < 3; ++c) {
+        if (!f->E[c] || !f->H[c] || !f->ce[c])
+            return fail(FDTD_ERR_INVALID, "field/coefficient pointer %d is NULL", c);
+        if (g->lossy && !f->ca[c]) return fail(FDTD_ERR_INVALID, "lossy grid without ca[%d]", c);
+        if (need_next) {
+            if (!f->E_next[c] || !f->H_next[c])
+                return fail(FDTD_ERR_INVALID, "E_next/H_next[%d] is NULL", c);
+            if (f->E_next[c] == f->E[c] || f->H_next[c] == f->H[c])
+                return fail(FDTD_ERR_INVALID, "fused step outputs must not alias inputs");
+        }
+    }
+    return FDTD_OK;
+}
+
+int check_cpml(const fdtd_grid *g, const fdtd_cpml *c, bool need_next) {
+    if (!c) return fail(FDTD_ERR_INVALID, "cpml is NULL");
+    for (int a = 0; a < 3; ++a)
+        if (!c->b_h[a] || !c->c_h[a] || !c->ik_h[a] || !c->b_e[a] || !c->c_e[a] || !c->ik_e[a])
+            return fail(FDTD_ERR_INVALID, "CPML profile pointer for axis %d is NULL", a);
+    if (g->npml > 0)
+        for (int q = 0; q < 6; ++q) {
+            if (!c->psi_h[q] || !c->psi_e[q])
+                return fail(FDTD_ERR_INVALID, "psi stripe %d is NULL", q);
+            if (need_next && (!c->psi_h_next[q] || c->psi_h_next[q] == c->psi_h[q]))
+                return fail(FDTD_ERR_INVALID, "psi_h_next[%d] is NULL or aliases psi_h", q);
+        }
+    return FDTD_OK;
+}
+
+int build_sources(const fdtd_grid *g, const fdtd_source *src, int nsrc, fdtd::SourceList &out) {
+    if (nsrc < 0 || nsrc > FDTD_MAX_SOURCES)
+        return fail(FDTD_ERR_INVALID, "nsrc must be in [0, %d], got %d", FDTD_MAX_SOURCES, nsrc);
+    if (nsrc > 0 && !src) return fail(FDTD_ERR_INVALID, "sources is NULL");
+    memset(&out, 0, sizeof(out));
+    out.n = nsrc;
+    for (int q = 0; q < nsrc; ++q) {
+        const fdtd_source &s = src[q];
+        if (s.kind != FDTD_SRC_JX && s.kind != FDTD_SRC_EX)
+            return fail(FDTD_ERR_INVALID, "source %d: unknown kind %d", q, s.kind);
+        if (s.z < 0 || s.z >= g->nz)
+            return fail(FDTD_ERR_INVALID, "source %d: z=%d outside [0, %d)", q, s.z, g->nz);
+        out.s[q] = s;
+    }
+    return FDTD_OK;
+}
+
+int build_planes(const fdtd_grid *g, const fdtd_plane_dft *pl, int np, fdtd::PlaneList &out) {
+    if (np < 0 || np > FDTD_MAX_PLANES)
+        return fail(FDTD_ERR_INVALID, "nplanes must be in [0, %d], got %d", FDTD_MAX_PLANES, np);
+    if (np > 0 && !pl) return fail(FDTD_ERR_INVALID, "planes is NULL");
+    memset(&out, 0, sizeof(out));
+    out.n = np;
+    const int dims[3] = {g->nx, g->ny, g->nz};
+    for (int q = 0; q < np; ++q) {
+        const fdtd_plane_dft &p = pl[q];
+        if (p.axis < 0 || p.axis > 2) return fail(FDTD_ERR_INVALID, "plane %d: axis %d", q, p.axis);
+        if (p.index < 0 || p.index >= dims[p.axis])
+            return fail(FDTD_ERR_INVALID, "plane %d: index %d outside [0, %d)", q, p.index,
+                        dims[p.axis]);
+        if (p.nfreq <= 0 || p.nfreq > FDTD_MAX_FREQS)
+            return fail(FDTD_ERR_INVALID, "plane %d: nfreq %d outside [1, %d]", q, p.nfreq,
+                        FDTD_MAX_FREQS);
+        if ((p.comp_mask & 0x3f) == 0 || (p.comp_mask & ~0x3f))
+            return fail(FDTD_ERR_INVALID, "plane %d: comp_mask 0x%x", q, p.comp_mask);
+        if (!p.acc || !p.phase) return fail(FDTD_ERR_INVALID, "plane %d: NULL buffer", q);
+        out.p[q] = p;
+    }
+    return FDTD_OK;
+}
+
+template <typename T>
+fdtd::YeeArgs<T> make_args(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c) {
+    fdtd::YeeArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.nx = g->nx;
+    a.ny = g->ny;
+    a.nz = g->nz;
+    a.npml = g->npml;
+    a.lossy = g->lossy ? 1 : 0;
+    a.dtm = (T)g->dtm;
+    a.dtm_dl = (T)g->dtm_dl;
+    a.inv_dl = (T)g->inv_dl;
+    for (int q = 0; q < 3; ++q) {
+        a.E[q] = (T *)f->E[q];
+        a.H[q] = (T *)f->H[q];
+        a.E_next[q] = (T *)f->E_next[q];
+        a.H_next[q] = (T *)f->H_next[q];
+        a.ce[q] = (const T *)f->ce[q];
+        a.ca[q] = (const T *)f->ca[q];
+        a.cph.b[q] = (const T *)c->b_h[q];
+        a.cph.c[q] = (const T *)c->c_h[q];
+        a.cph.ik[q] = (const T *)c->ik_h[q];
+        a.cpe.b[q] = (const T *)c->b_e[q];
+        a.cpe.c[q] = (const T *)c->c_e[q];
+        a.cpe.ik[q] = (const T *)c->ik_e[q];
+    }
+    for (int q = 0; q < 6; ++q) {
+        a.psi_h[q] = (T *)c->psi_h[q];
+        a.psi_h_next[q] = (T *)c->psi_h_next[q];
+        a.psi_e[q] = (T *)c->psi_e[q];
+    }
+    return a;
+}
+
+int check_box(const fdtd_grid *g, const fdtd_box *b) {
+    if (!b) return fail(FDTD_ERR_INVALID, "box is NULL");
+    if (g && (b->ix0 < 0 || b->ix1 >= g->nx || b->ix0 > b->ix1 || b->iy0 < 0 || b->iy1 >= g->ny ||
+        b->iy0 > b->iy1 || b->iz0 < 0 || b->iz1 >= g->nz || b->iz0 > b->iz1))
+        return fail(FDTD_ERR_INVALID, "box (%d..%d, %d..%d, %d..%d) outside the grid", b->ix0,
+                    b->ix1, b->iy0, b->iy1, b->iz0, b->iz1);
+    if (b->ix0 > b->ix1 || b->iy0 > b->iy1 || b->iz0 > b->iz1)
+        return fail(FDTD_ERR_INVALID, "box is empty");
+    const int64_t nxf = b->ix1 - b->ix0 + 1, nyf = b->iy1 - b->iy0 + 1, nzf = b->iz1 - b->iz0 + 1;
+    const int64_t cnt[6] = {nyf * nzf, nyf * nzf, nxf * nzf, nxf * nzf, nxf * nyf, nxf * nyf};
+    int64_t o = 0;
+    for (int q = 0; q < 6; ++q) {
+        if (b->off[q] != o) return fail(FDTD_ERR_INVALID, "box face offset %d is %d, expected %lld",
+                                        q, b->off[q], (long long)o);
+        o += cnt[q];
+    }
+    if (b->n_face != o) return fail(FDTD_ERR_INVALID, "box n_face %d, expected %lld", b->n_face,
+                                    (long long)o);
+    if (b->nfreq <= 0 || b->nfreq > FDTD_MAX_FREQS)
+        return fail(FDTD_ERR_INVALID, "box nfreq %d outside [1, %d]", b->nfreq, FDTD_MAX_FREQS);
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fdtd_last_error(void) { return g_err.c_str(); }
+
+const char *fdtd_version(void) { return "fdtd_b200 0.1 sm_100a"; }
+
+int fdtd_device_status(int32_t *flags, int32_t reset) {
+    if (!flags) return fail(FDTD_ERR_INVALID, "flags is NULL");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "device_status");
+    *flags = fdtd::read_fused_error(reset);
+    return cuda_status(cudaGetLastError(), "device_status");
+}
+
+int fdtd_update_H(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c, void *stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c, false)))
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_update_H<float>(make_args<float>(g, f, c), st), "update_H");
+    return cuda_status(fdtd::launch_update_H<double>(make_args<double>(g, f, c), st), "update_H");
+}
+
+int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
+                  const fdtd_source *src, int32_t nsrc, const fdtd_plane_dft *planes,
+                  int32_t nplanes, void *stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c, false)))
+        return rc;
+    fdtd::SourceList sl;
+    fdtd::PlaneList pl;
+    if ((rc = build_sources(g, src, nsrc, sl)) || (rc = build_planes(g, planes, nplanes, pl)))
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_update_E<float>(make_args<float>(g, f, c), sl, pl, st),
+                           "update_E");
+    return cuda_status(fdtd::launch_update_E<double>(make_args<double>(g, f, c), sl, pl, st),
+                       "update_E");
+}
+
+int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
+              const fdtd_source *src, int32_t nsrc, const fdtd_plane_dft *planes,
+              int32_t nplanes, void *stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, true)) || (rc = check_cpml(g, c, true)))
+        return rc;
+    fdtd::SourceList sl;
+    fdtd::PlaneList pl;
+    if ((rc = build_sources(g, src, nsrc, sl)) || (rc = build_planes(g, planes, nplanes, pl)))
+        return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_step_fused<float>(make_args<float>(g, f, c), sl, pl, st),
+                           "step");
+    return cuda_status(fdtd::launch_step_fused<double>(make_args<double>(g, f, c), sl, pl, st),
+                       "step");
+}
+
+int fdtd_add_source(const fdtd_grid *g, void *Ex, const void *ce_x, const fdtd_source *src,
+                    void *stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!Ex || !ce_x) return fail(FDTD_ERR_INVALID, "Ex/ce_x is NULL");
+    fdtd::SourceList sl;
+    if ((rc = build_sources(g, src, 1, sl))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_add_source<float>(g->nx, g->ny, g->nz, *src, (float *)Ex,
+                                                          (const float *)ce_x, st),
+                           "add_source");
+    return cuda_status(fdtd::launch_add_source<double>(g->nx, g->ny, g->nz, *src, (double *)Ex,
+                                                       (const double *)ce_x, st),
+                       "add_source");
+}
+
+int fdtd_dft_faces(const fdtd_grid *g, const void *const E[3], const void *const H[3],
+                   const fdtd_box *box, double *acc, const double *phase, void *stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_box(g, box))) return rc;
+    if (!E || !H || !acc || !phase) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    for (int q = 0; q < 3; ++q)
+        if (!E[q] || !H[q]) return fail(FDTD_ERR_INVALID, "NULL field %d", q);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32) {
+        const float *e[3] = {(const float *)E[0], (const float *)E[1], (const float *)E[2]};
+        const float *h[3] = {(const float *)H[0], (const float *)H[1], (const float *)H[2]};
+        return cuda_status(fdtd::launch_dft_faces<float>(g->nx, g->ny, g->nz, e, h, *box, acc,
+                                                         phase, st),
+                           "dft_faces");
+    }
+    const double *e[3] = {(const double *)E[0], (const double *)E[1], (const double *)E[2]};
+    const double *h[3] = {(const double *)H[0], (const double *)H[1], (const double *)H[2]};
+    return cuda_status(
+        fdtd::launch_dft_faces<double>(g->nx, g->ny, g->nz, e, h, *box, acc, phase, st),
+        "dft_faces");
+}
+
+int fdtd_rel_change_blocks(int32_t n_face) { return fdtd::rel_change_blocks(n_face); }
+
+int fdtd_dft_rel_change(const double *cur, const double *prev, int32_t n_face, int32_t nfreq,
+                        int32_t fi, double *scratch, double *out2, void *stream) {
+    if (!cur || !prev || !scratch || !out2) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    if (n_face <= 0 || nfreq <= 0 || fi < 0 || fi >= nfreq)
+        return fail(FDTD_ERR_INVALID, "n_face %d, nfreq %d, fi %d", n_face, nfreq, fi);
+    return cuda_status(fdtd::launch_rel_change(cur, prev, n_face, nfreq, fi, scratch, out2,
+                                               (cudaStream_t)stream),
+                       "dft_rel_change");
+}
+
+int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl, double k_wave,
+                  double eta0, const double *obs_xyz, int32_t n_obs, double *nl_scratch,
+                  double *eh, void *stream) {
+    if (!box || !acc || !obs_xyz || !nl_scratch || !eh)
+        return fail(FDTD_ERR_INVALID, "NULL buffer");
+    int rc;
+    if ((rc = check_box(nullptr, box))) return rc;
+    if (n_obs <= 0) return fail(FDTD_ERR_INVALID, "n_obs must be positive, got %d", n_obs);
+    if (fi < 0 || fi >= box->nfreq)
+        return fail(FDTD_ERR_INVALID, "frequency index %d outside [0, %d)", fi, box->nfreq);
+    if (!(dl > 0) || !(k_wave >= 0) || !(eta0 > 0))
+        return fail(FDTD_ERR_INVALID, "dl, k_wave, eta0 must be positive");
+    return cuda_status(fdtd::launch_farfield(*box, acc, fi, dl, k_wave, eta0, obs_xyz, n_obs,
+                                             nl_scratch, eh, (cudaStream_t)stream),
+                       "farfield");
+}
+
+}  // extern "C"

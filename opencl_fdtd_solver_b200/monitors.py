@@ -1,0 +1,350 @@
+"""GPU DFT monitors for ``CUDAFDTD``.
+
+``CUDANear2FarMonitor`` keeps the surface of the reference ``OpenCLNear2FarMonitor``
+(``opencl_fdtd_solver/monitors.py:383-804``): box snapping (``:37-45``), packed faces
+x0,x1,y0,y1,z0,z1 (``:396-412``), per-step phase recurrence (``:456-459, 571-584``),
+``get_farfield(s)`` (``:644-735``), ``farfield_polar_xz`` (``:737-755``),
+``snapshot_dft`` / ``dft_relative_change`` (``:487-569``) and ``fetch_dft_fields``
+(``:757-804``).  It additionally accepts a list of frequencies (one accumulator
+slice per frequency); a scalar ``freq`` keeps the reference form.  Far fields use
+the reference kernel's sign ``η·N⊥ − r̂×L`` (``dft_farfield.cl:617``).
+
+``CUDAPlaneDFTMonitor`` has no reference class: a running DFT of chosen field
+components on one grid plane, accumulated inside the E-update kernel (no extra
+pass over the fields), with the same phase convention (E at the step time, H half
+a step earlier).
+
+Accumulators are complex128 on the device; the phase recurrence is evaluated on
+the host in complex128 exactly as the reference does and uploaded in chunks.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _capi as capi
+from .constants import C0, ETA0
+
+FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+_PHASE_CHUNK = 512
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class _PhaseTable:
+    """Device table of the per-step phases ``[chunk][nfreq][4]`` (E re, E im, H re, H im).
+
+    The first call uses ``e^{jωt}·dt``; later calls multiply by ``e^{jωdt}``
+    (reference ``monitors.py:571-577``), computed ahead a chunk at a time.
+    """
+
+    def __init__(self, freqs, dt, device):
+        self.omega = 2.0 * np.pi * np.asarray(freqs, dtype=np.float64)
+        self.dt = float(dt)
+        self.dphase = np.exp(1j * self.omega * self.dt)
+        self.half = np.exp(-0.5j * self.omega * self.dt)
+        self.device = device
+        self.phase = None  # host value of the most recent step (complex128 [nfreq])
+        self._host = None
+        self._dev = None
+        self._cursor = 0
+
+    def _fill(self, first):
+        nf = self.omega.size
+        host = np.empty((_PHASE_CHUNK, nf, 4), np.float64)
+        p = first
+        seq = np.empty((_PHASE_CHUNK, nf), np.complex128)
+        for s in range(_PHASE_CHUNK):
+            if s > 0:
+                p = p * self.dphase
+            seq[s] = p
+        ph = seq * self.half
+        host[:, :, 0], host[:, :, 1] = seq.real, seq.imag
+        host[:, :, 2], host[:, :, 3] = ph.real, ph.imag
+        self._seq = seq
+        torch = _torch()
+        self._dev = torch.from_numpy(host).to(self.device)
+        self._cursor = 0
+
+    def next_ptr(self, t):
+        """Advance one step (monitor time ``t``) and return the device pointer of its phases."""
+        if self._dev is None:
+            self._fill(np.exp(1j * self.omega * t) * self.dt)
+        elif self._cursor >= _PHASE_CHUNK:
+            self._fill(self._seq[-1] * self.dphase)
+        s = self._cursor
+        self.phase = self._seq[s]
+        self._cursor += 1
+        return self._dev.data_ptr() + s * self.omega.size * 4 * 8
+
+
+class CUDAPlaneDFTMonitor:
+    """Running DFT of ``components`` on the plane ``axis = index`` at ``freqs``.
+
+    ``axis`` is 0/1/2 or ``'x'/'y'/'z'``.  Accumulated in the E-update kernel; the
+    result ``dft(c)`` has shape ``(n_freq, n1, n2)`` over the two other axes in
+    C order.  Registers itself on ``fdtd`` (at most four per engine).
+    """
+
+    def __init__(self, fdtd, axis, index, freqs, components=("Ex",)):
+        torch = _torch()
+        self.fdtd = fdtd
+        self.axis = {"x": 0, "y": 1, "z": 2}.get(axis, axis)
+        if self.axis not in (0, 1, 2):
+            raise ValueError(f"axis must be 0, 1, 2 or 'x', 'y', 'z'; got {axis!r}")
+        dims = [fdtd.Nx, fdtd.Ny, fdtd.Nz]
+        self.index = int(index)
+        if not 0 <= self.index < dims[self.axis]:
+            raise ValueError(f"plane index {index} outside [0, {dims[self.axis]})")
+        self.freqs = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+        if not 0 < self.freqs.size <= capi.FDTD_MAX_FREQS:
+            raise ValueError(f"1 to {capi.FDTD_MAX_FREQS} frequencies, got {self.freqs.size}")
+        comps = (components,) if isinstance(components, str) else tuple(components)
+        for c in comps:
+            if c not in FIELDS:
+                raise ValueError(f"unknown component {c!r}")
+        # stored in Ex..Hz order (the kernel's slot order)
+        self.components = tuple(c for c in FIELDS if c in comps)
+        self.comp_mask = sum(1 << FIELDS.index(c) for c in self.components)
+        del dims[self.axis]
+        self.plane_shape = tuple(dims)
+        with torch.cuda.stream(fdtd.queue):
+            self.acc = torch.zeros((len(self.components), self.freqs.size, *dims, 2),
+                                   dtype=torch.float64, device=fdtd.device)
+        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device)
+        n_planes = sum(1 for m in fdtd._monitors if isinstance(m, CUDAPlaneDFTMonitor))
+        if n_planes >= capi.FDTD_MAX_PLANES:
+            raise ValueError(f"at most {capi.FDTD_MAX_PLANES} plane DFT monitors per engine")
+        fdtd.add_monitor(self)
+
+    @property
+    def _phase(self):
+        return self._phases.phase
+
+    def _descriptor(self, t_next):
+        d = capi.PlaneDft()
+        d.axis, d.index, d.comp_mask, d.nfreq = self.axis, self.index, self.comp_mask, \
+            self.freqs.size
+        d.acc = self.acc.data_ptr()
+        d.phase = self._phases.next_ptr(t_next)
+        return d
+
+    def __call__(self, fdtd):
+        # accumulation happened inside the E update of this step
+        return None
+
+    def dft_tensor(self):
+        """Device view ``complex128 [n_comp, n_freq, n1, n2]``."""
+        return _torch().view_as_complex(self.acc)
+
+    def dft(self, component=None):
+        """Host ``complex128`` array ``(n_freq, n1, n2)`` for one component (default: first)."""
+        c = self.components[0] if component is None else component
+        q = self.components.index(c)
+        self.fdtd.queue.synchronize()
+        a = self.acc[q].cpu().numpy()
+        return a[..., 0] + 1j * a[..., 1]
+
+
+class CUDANear2FarMonitor:
+    """Huygens-box DFT + near-to-far transform on the GPU (``OpenCLNear2FarMonitor`` API)."""
+
+    def __init__(self, fdtd, center, size, freq):
+        torch = _torch()
+        self.fdtd = fdtd
+        self.freqs = np.atleast_1d(np.asarray(freq, dtype=np.float64))
+        if not 0 < self.freqs.size <= capi.FDTD_MAX_FREQS:
+            raise ValueError(f"1 to {capi.FDTD_MAX_FREQS} frequencies, got {self.freqs.size}")
+        self.freq = float(self.freqs[0]) if np.ndim(freq) == 0 else self.freqs
+        self.omega = 2.0 * np.pi * self.freq if np.ndim(freq) == 0 else 2.0 * np.pi * self.freqs
+        self.dl = fdtd.dl
+        cx, cy, cz = center
+        sx, sy, sz = size
+
+        def _idx(phys):
+            return int(round(phys / fdtd.dl))
+
+        self.ix0 = max(0, _idx(cx - sx / 2))
+        self.ix1 = min(fdtd.Nx - 1, _idx(cx + sx / 2))
+        self.iy0 = max(0, _idx(cy - sy / 2))
+        self.iy1 = min(fdtd.Ny - 1, _idx(cy + sy / 2))
+        self.iz0 = max(0, _idx(cz - sz / 2))
+        self.iz1 = min(fdtd.Nz - 1, _idx(cz + sz / 2))
+        if self.ix0 > self.ix1 or self.iy0 > self.iy1 or self.iz0 > self.iz1:
+            raise ValueError("Huygens box is empty after snapping to the grid")
+        self._box = (self.ix0, self.ix1, self.iy0, self.iy1, self.iz0, self.iz1)
+        self.nxf = self.ix1 - self.ix0 + 1
+        self.nyf = self.iy1 - self.iy0 + 1
+        self.nzf = self.iz1 - self.iz0 + 1
+        self._face_counts = (self.nyf * self.nzf, self.nyf * self.nzf, self.nxf * self.nzf,
+                             self.nxf * self.nzf, self.nxf * self.nyf, self.nxf * self.nyf)
+        offs = [0]
+        for c in self._face_counts[:-1]:
+            offs.append(offs[-1] + c)
+        self._face_offsets = tuple(offs)
+        self.n_face_samples = int(sum(self._face_counts))
+        self._dtype = fdtd.dtype
+        self._acc_complex_dtype = fdtd.accreal_complex_dtype
+        b = capi.Box()
+        b.ix0, b.ix1, b.iy0, b.iy1, b.iz0, b.iz1 = self._box
+        for q in range(6):
+            b.off[q] = self._face_offsets[q]
+        b.n_face = self.n_face_samples
+        b.nfreq = self.freqs.size
+        self._cbox = b
+        with torch.cuda.stream(fdtd.queue):
+            self.acc = torch.zeros((6, self.freqs.size, self.n_face_samples, 2),
+                                   dtype=torch.float64, device=fdtd.device)
+        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device)
+        self._dft_snap = None
+        self.Ex_dft = self.Ey_dft = self.Ez_dft = None
+        self.Hx_dft = self.Hy_dft = self.Hz_dft = None
+        fdtd.add_monitor(self)
+
+    @property
+    def _phase(self):
+        p = self._phases.phase
+        if p is None:
+            return None
+        return complex(p[0]) if np.ndim(self.freq) == 0 else p
+
+    def __call__(self, fdtd):
+        ptr = self._phases.next_ptr(fdtd.t)
+        E = (capi.c_void_p * 3)(*[t.data_ptr() for t in fdtd._E])
+        H = (capi.c_void_p * 3)(*[t.data_ptr() for t in fdtd._H])
+        capi.run("fdtd_dft_faces", fdtd._grid, E, H, self._cbox, self.acc.data_ptr(), ptr,
+                 fdtd.queue.cuda_stream)
+
+    # ------------------------------------------------------------ far field
+    def _fi(self, freq_index):
+        fi = int(freq_index)
+        if not 0 <= fi < self.freqs.size:
+            raise IndexError(f"frequency index {fi} outside [0, {self.freqs.size})")
+        return fi
+
+    def get_farfields(self, obs_points, freq_index=0) -> np.ndarray:
+        """Far E, H at many points (metres): ``(n_obs, 6)`` complex128 (Ex, Ey, Ez, Hx, Hy, Hz)."""
+        torch = _torch()
+        pts = np.asarray(obs_points, dtype=self._dtype)
+        if pts.ndim == 1:
+            pts = pts.reshape(1, 3)
+        if pts.ndim != 2 or pts.shape[1] != 3:
+            raise ValueError("obs_points must be (n,3) or (3,)")
+        fi = self._fi(freq_index)
+        n_obs = int(pts.shape[0])
+        q = self.fdtd.queue
+        with torch.cuda.stream(q):
+            obs = torch.from_numpy(pts.astype(np.float64)).to(self.fdtd.device)
+            nl = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=self.fdtd.device)
+            eh = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=self.fdtd.device)
+        k_wave = 2.0 * np.pi * float(self.freqs[fi]) / C0
+        capi.run("fdtd_farfield", self._cbox, self.acc.data_ptr(), fi, float(self.dl), k_wave,
+                 float(ETA0), obs.data_ptr(), n_obs, nl.data_ptr(), eh.data_ptr(), q.cuda_stream)
+        q.synchronize()
+        h = eh.cpu().numpy()
+        return (h[..., 0] + 1j * h[..., 1]).astype(np.complex128)
+
+    def get_farfield(self, obs_point, freq_index=0):
+        """Far E, H at one point (metres)."""
+        return self.get_farfields([obs_point], freq_index)[0]
+
+    def farfield_polar_xz(self, *, distance_m: float = 1000.0, n_angles: int = 73,
+                          freq_index: int = 0):
+        """XZ-plane cut: ``(angles_deg, |S| dB)`` at ``distance_m``."""
+        R = float(distance_m)
+        if R <= 0.0:
+            raise ValueError("distance_m must be positive")
+        n = max(3, int(n_angles))
+        angles = np.linspace(-180.0, 180.0, n, dtype=np.float64)
+        rad = np.deg2rad(angles)
+        pts = np.column_stack([R * np.sin(rad), np.zeros(n), R * np.cos(rad)]).astype(self._dtype)
+        eh = self.get_farfields(pts, freq_index)
+        db = np.empty(n, dtype=np.float64)
+        for i in range(n):
+            db[i], _ = _poynting_db(eh[i])
+        return angles, db
+
+    # ----------------------------------------------------- DFT convergence
+    def snapshot_dft(self) -> None:
+        """Copy the face DFTs to a device snapshot (no host round trip)."""
+        torch = _torch()
+        with torch.cuda.stream(self.fdtd.queue):
+            if self._dft_snap is None:
+                self._dft_snap = torch.empty_like(self.acc)
+            self._dft_snap.copy_(self.acc)
+
+    def dft_relative_change(self, freq_index=0) -> float:
+        """``‖cur − prev‖₂ / ‖cur‖₂`` over the six face DFTs (1.0 without a snapshot)."""
+        if self._dft_snap is None:
+            return 1.0
+        torch = _torch()
+        fi = self._fi(freq_index)
+        q = self.fdtd.queue
+        nblk = int(capi.lib().fdtd_rel_change_blocks(self.n_face_samples))
+        with torch.cuda.stream(q):
+            scratch = torch.empty(2 * nblk, dtype=torch.float64, device=self.fdtd.device)
+            out = torch.empty(2, dtype=torch.float64, device=self.fdtd.device)
+        capi.run("fdtd_dft_rel_change", self.acc.data_ptr(), self._dft_snap.data_ptr(),
+                 self.n_face_samples, self.freqs.size, fi, scratch.data_ptr(), out.data_ptr(),
+                 q.cuda_stream)
+        q.synchronize()
+        num, den = (float(v) for v in out.cpu().numpy())
+        if den <= 0.0 or not np.isfinite(den) or not np.isfinite(num):
+            return 1.0
+        return float(np.sqrt(max(num, 0.0) / den))
+
+    # ----------------------------------------------------------- download
+    def face_dft(self, freq_index=0):
+        """Face-packed complex128 DFTs ``{name: (n_face,)}`` for one frequency."""
+        fi = self._fi(freq_index)
+        self.fdtd.queue.synchronize()
+        a = self.acc[:, fi].cpu().numpy()
+        return {n: a[q, :, 0] + 1j * a[q, :, 1] for q, n in enumerate(FIELDS)}
+
+    def fetch_dft_fields(self, freq_index=0):
+        """Download face DFTs and scatter them into sparse host volumes ``Ex_dft``…``Hz_dft``."""
+        faces = {k: v.astype(self._acc_complex_dtype) for k, v in
+                 self.face_dft(freq_index).items()}
+        shape = (self.fdtd.Nx, self.fdtd.Ny, self.fdtd.Nz)
+
+        def scatter(face_arr):
+            vol = np.zeros(shape, dtype=self._acc_complex_dtype)
+            for fid, ii in ((0, self.ix0), (1, self.ix1)):
+                b = self._face_offsets[fid]
+                vol[ii, self.iy0:self.iy1 + 1, self.iz0:self.iz1 + 1] = \
+                    face_arr[b:b + self.nyf * self.nzf].reshape(self.nyf, self.nzf)
+            for fid, jj in ((2, self.iy0), (3, self.iy1)):
+                b = self._face_offsets[fid]
+                vol[self.ix0:self.ix1 + 1, jj, self.iz0:self.iz1 + 1] = \
+                    face_arr[b:b + self.nxf * self.nzf].reshape(self.nxf, self.nzf)
+            for fid, kk in ((4, self.iz0), (5, self.iz1)):
+                b = self._face_offsets[fid]
+                vol[self.ix0:self.ix1 + 1, self.iy0:self.iy1 + 1, kk] = \
+                    face_arr[b:b + self.nxf * self.nyf].reshape(self.nxf, self.nyf)
+            return vol
+
+        for n in FIELDS:
+            setattr(self, f"{n}_dft", scatter(faces[n]))
+        return faces
+
+
+def _poynting_mag(ff) -> float:
+    """``|½ E × H*|`` of a 6-vector (reference ``monitors.py:807-813``)."""
+    E = ff[0:3]
+    H = ff[3:6]
+    Sx = 0.5 * (E[1] * np.conj(H[2]) - E[2] * np.conj(H[1]))
+    Sy = 0.5 * (E[2] * np.conj(H[0]) - E[0] * np.conj(H[2]))
+    Sz = 0.5 * (E[0] * np.conj(H[1]) - E[1] * np.conj(H[0]))
+    return float(np.sqrt(np.abs(Sx) ** 2 + np.abs(Sy) ** 2 + np.abs(Sz) ** 2))
+
+
+def _poynting_db(ff) -> tuple[float, float]:
+    """``(20·log10|S|, |S|)``, ``-inf`` for zero or non-finite (``monitors.py:816-827``)."""
+    mag = _poynting_mag(ff)
+    if not np.isfinite(mag) or mag <= 0.0:
+        return float("-inf"), 0.0
+    return float(20.0 * np.log10(mag)), mag
