@@ -68,7 +68,8 @@ typedef struct {
  * staggers (cpml.py:111-134, engine.py:264-283), and the 12 ψ stripes.
  * psi_h order: Hx_y, Hx_z, Hy_x, Hy_z, Hz_x, Hz_y;
  * psi_e order: Ex_y, Ex_z, Ey_x, Ey_z, Ez_x, Ez_y (yee_update.cl:56-58,176-178).
- * psi_h_next receives the fused step's ψ_H (must not alias psi_h). */
+ * Every entry point updates the ψ stripes in place; psi_h_next is reserved
+ * (ignored, may be NULL). */
 typedef struct {
     const void *b_h[3], *c_h[3], *ik_h[3];
     const void *b_e[3], *c_e[3], *ik_e[3];
@@ -116,8 +117,10 @@ int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
                   const fdtd_source *src, int32_t nsrc,
                   const fdtd_plane_dft *planes, int32_t nplanes, void *stream);
 
-/* One full leapfrog step H -> sources -> E in a single pass over HBM:
- * reads E/H/psi_h, writes E_next/H_next/psi_h_next (psi_e in place).
+/* One full leapfrog step H -> sources -> E: reads E/H, writes E_next/H_next,
+ * ψ stripes in place.  The interior box [npml, N-npml)^3 is updated by one
+ * single-pass kernel (H and E per plane, one read and one write of each array);
+ * the CPML shell around it by per-cell H and E kernels before and after it.
  * Replaces the whole of OpenCLFDTD.step() up to the monitors
  * (engine.py:724-735): _update_H, the source callbacks' injections, _update_E. */
 int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,

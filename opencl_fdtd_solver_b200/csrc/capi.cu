@@ -76,7 +76,7 @@ int check_fields(const fdtd_grid *g, const fdtd_fields *f, bool need_next) {
     return FDTD_OK;
 }
 
-int check_cpml(const fdtd_grid *g, const fdtd_cpml *c, bool need_next) {
+int check_cpml(const fdtd_grid *g, const fdtd_cpml *c) {
     if (!c) return fail(FDTD_ERR_INVALID, "cpml is NULL");
     for (int a = 0; a < 3; ++a)
         if (!c->b_h[a] || !c->c_h[a] || !c->ik_h[a] || !c->b_e[a] || !c->c_e[a] || !c->ik_e[a])
@@ -85,8 +85,6 @@ int check_cpml(const fdtd_grid *g, const fdtd_cpml *c, bool need_next) {
         for (int q = 0; q < 6; ++q) {
             if (!c->psi_h[q] || !c->psi_e[q])
                 return fail(FDTD_ERR_INVALID, "psi stripe %d is NULL", q);
-            if (need_next && (!c->psi_h_next[q] || c->psi_h_next[q] == c->psi_h[q]))
-                return fail(FDTD_ERR_INVALID, "psi_h_next[%d] is NULL or aliases psi_h", q);
         }
     return FDTD_OK;
 }
@@ -207,7 +205,7 @@ int fdtd_device_status(int32_t *flags, int32_t reset) {
 
 int fdtd_update_H(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c, void *stream) {
     int rc;
-    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c, false)))
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c)))
         return rc;
     cudaStream_t st = (cudaStream_t)stream;
     if (g->dtype == FDTD_F32)
@@ -219,7 +217,7 @@ int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
                   const fdtd_source *src, int32_t nsrc, const fdtd_plane_dft *planes,
                   int32_t nplanes, void *stream) {
     int rc;
-    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c, false)))
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, false)) || (rc = check_cpml(g, c)))
         return rc;
     fdtd::SourceList sl;
     fdtd::PlaneList pl;
@@ -237,7 +235,7 @@ int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
               const fdtd_source *src, int32_t nsrc, const fdtd_plane_dft *planes,
               int32_t nplanes, void *stream) {
     int rc;
-    if ((rc = check_grid(g)) || (rc = check_fields(g, f, true)) || (rc = check_cpml(g, c, true)))
+    if ((rc = check_grid(g)) || (rc = check_fields(g, f, true)) || (rc = check_cpml(g, c)))
         return rc;
     fdtd::SourceList sl;
     fdtd::PlaneList pl;

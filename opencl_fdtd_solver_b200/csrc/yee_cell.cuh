@@ -193,6 +193,17 @@ struct PlaneList {
     int n;
 };
 
+// True when cell (i, j, k) lies on one of the DFT planes (integer tests only,
+// so the per-cell cost away from the planes is a few compares).
+__device__ __forceinline__ bool plane_any_hit(const PlaneList &pl, int i, int j, int k) {
+    bool hit = false;
+    for (int q = 0; q < pl.n; ++q) {
+        const fdtd_plane_dft &p = pl.p[q];
+        hit |= (p.axis == 0) ? (i == p.index) : (p.axis == 1) ? (j == p.index) : (k == p.index);
+    }
+    return hit;
+}
+
 // Accumulate the plane DFTs that contain cell (i, j, k).  v[0..5] are the
 // cell's Ex, Ey, Ez (at step n+1) and Hx, Hy, Hz (at n+1/2).
 __device__ __forceinline__ void plane_dft_cell(const PlaneList &pl, int i, int j, int k, int nx,
@@ -214,6 +225,7 @@ __device__ __forceinline__ void plane_dft_cell(const PlaneList &pl, int i, int j
             ncell = (int64_t)nx * ny;
         }
         int slot = 0;
+#pragma unroll
         for (int c = 0; c < 6; ++c) {
             if (!(p.comp_mask & (1 << c))) continue;
             const int h = c >= 3 ? 2 : 0;

@@ -1,36 +1,46 @@
-// Fused single-pass Yee step for sm_100a: H^{n-1/2} -> H^{n+1/2}, sheet
-// injections, E^n -> E^{n+1} and plane DFTs in one sweep over HBM.
+// Fused Yee step for sm_100a: one pass over HBM for the interior of the grid.
 //
-// Schedule.  Each CTA owns a (TJ x TK) tile of (j, k) and marches along i over
-// a chunk of planes [i0, i1).  Plane p of the input fields is brought into
-// shared memory by TMA (cp.async.bulk.tensor, 3-D tiled maps, no multicast):
-//   E^n(p)       rows j0-1 .. j0+TJ, cols k0-HP .. k0+TK+HP-1  (1-cell halo;
-//                the k extent is widened to 16-byte boundaries)
-//   H^{n-1/2}(p) rows j0-1 .. j0+TJ-1, cols k0-HP .. k0+TK-1
-//   ce(p) [ca(p)] the tile only
-// through an NSTAGE-deep ring of stages, each completed by one mbarrier with a
-// transaction-byte count.  Per plane the CTA computes H^{n+1/2}(p) on the tile
-// plus the j0-1 row and k0-1 column that the E stencil needs (recomputed from
-// the same inputs, so no inter-CTA exchange), then E^{n+1}(p) on the tile from
-// H^{n+1/2}(p) (shared memory) and H^{n+1/2}(p-1) (carried in registers).
-// Outputs go to separate buffers (E_next, H_next, psi_h_next), so no CTA ever
-// reads a value another CTA has already overwritten; psi_e is per-cell and
-// updated in place.  A chunk starting at i0 > 0 first recomputes
-// H^{n+1/2}(i0-1) for its tile (no stores).
+// Schedule of fdtd_step (three launches on one stream):
+//   1. k_shell_H   (yee_shell.cu): H^{n+1/2} on the CPML shell outside the box
+//                  B = [npml, N-npml)^3, psi_H in place, into H_next.
+//   2. k_interior  (this file): H^{n+1/2} on B and E^{n+1} on B' = [npml+1,
+//                  N-npml)^3, into H_next / E_next, sheet injections of those
+//                  cells in the E epilogue.  Every H value its E
+//                  stencil needs lies in B and is recomputed here, so it never
+//                  waits for the shell.
+//   3. k_plane_dft_box (yee_shell.cu, only with plane DFT monitors): the DFTs of
+//                  the monitored planes' cells inside B', read back from the
+//                  values just written (one plane, not a field pass).
+//   4. k_shell_E   (yee_shell.cu): E^{n+1} outside B' from the final H_next,
+//                  with the injections and plane DFTs of those cells.
 //
-// HBM traffic per cell: E, H, ce read once and E, H written once (60 B in FP32
-// lossless), plus the CPML stripes and the plane-DFT accumulators.
+// Interior kernel.  Each CTA owns a (TJ x TK) tile of (j, k) and marches along
+// i over a chunk of planes.  Plane p is brought into shared memory by TMA
+// (cp.async.bulk.tensor 3-D tiled maps, no multicast) through an NSTAGE-deep
+// ring completed by mbarrier transaction counts:
+//   E^n(p)       rows j0-1 .. j0+TJ,  cols k0-V .. k0+TK+V-1   (V = 16 B / elem)
+//   H^{n-1/2}(p) rows j0-1 .. j0+TJ-1, cols k0-V .. k0+TK-1
+//   ce(p) [ca(p)] the tile only.
+// Per plane the 128 "cell" threads each update V consecutive k cells (16-byte
+// vector shared-memory loads and global stores) and a fifth "halo" warp
+// recomputes the j0-1 row and k0-1 column of H^{n+1/2}; E^{n+1} then uses
+// H^{n+1/2}(p) from shared memory and H^{n+1/2}(p-1) carried in registers.
+// Interior cells need no CPML terms and no boundary guards, so the per-cell
+// work is the folded-coefficient update of yee_update.cl:30-39 / 145-154.
+// HBM traffic per interior cell: E, H, ce read once, E, H written once
+// (60 B FP32 lossless); outputs go to separate buffers, so no CTA reads a value
+// another has overwritten.
 //
-// Arithmetic: the per-cell expressions are those of yee_cell.cuh, compiled
-// with --fmad=false, so results equal the split kernels and the CPU oracle bit
-// for bit.
-//
+// Arithmetic is compiled with --fmad=false and follows the reference operand
+// order, so every cell equals the split kernels and the CPU oracle bit for bit.
 // Every mbarrier wait is bounded; on timeout the kernel raises a device error
 // flag, drains its outstanding copies (bounded again) and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -42,8 +52,9 @@ namespace fdtd {
 
 __device__ int g_fused_error = 0;
 
-constexpr int NSTAGE = 4;
-constexpr int NTHREADS = 256;
+constexpr int NSTAGE_DEFAULT = 4;  // pipeline depth (planes in flight + 2)
+constexpr int NCELLTHR = 128;             // 16 vector groups x 8 rows
+constexpr int NTHREADS = NCELLTHR + 32;  // + one halo warp
 constexpr unsigned WAIT_LIMIT = 1u << 24;
 
 struct alignas(64) FusedMaps {
@@ -54,15 +65,24 @@ struct alignas(64) FusedMaps {
 };
 
 template <typename T>
-struct FusedTile {
-    static constexpr int TK = (sizeof(T) == 4) ? 64 : 32;  // 256-byte rows
-    static constexpr int TJ = 8;
-    static constexpr int HP = 16 / (int)sizeof(T);         // 16-byte k alignment pad
-    static constexpr int NTY = NTHREADS / TK;
-    static constexpr int RPT = TJ / NTY;                    // rows per thread
-    static constexpr int EW = TK + 2 * HP, EH = TJ + 2;
-    static constexpr int HW = TK + HP, HH = TJ + 1;
-    static constexpr int NW = TK + 1, NH = TJ + 1;          // new-H plane incl. halo
+struct VecT;
+template <>
+struct VecT<float> {
+    using type = float4;
+};
+template <>
+struct VecT<double> {
+    using type = double2;
+};
+
+template <typename T>
+struct Tile {
+    static constexpr int V = 16 / (int)sizeof(T);  // elements per 16-byte vector
+    static constexpr int G = 16;                    // vector groups per row
+    static constexpr int TK = G * V;                // 64 (FP32) or 32 (FP64)
+    static constexpr int TJ = NCELLTHR / G;         // 8
+    static constexpr int EW = TK + 2 * V, EH = TJ + 2;
+    static constexpr int HW = TK + V, HH = TJ + 1;
     __host__ __device__ static constexpr int pad128(int b) { return (b + 127) / 128 * 128; }
     static constexpr int EB = pad128(EW * EH * (int)sizeof(T));
     static constexpr int HB = pad128(HW * HH * (int)sizeof(T));
@@ -70,11 +90,7 @@ struct FusedTile {
     __host__ __device__ static constexpr int stage_bytes(bool lossy) {
         return 3 * EB + 3 * HB + 3 * CB * (lossy ? 2 : 1);
     }
-    static constexpr int NB = pad128(3 * NW * NH * (int)sizeof(T));
-    __host__ __device__ static constexpr int smem_bytes(bool lossy) {
-        return NSTAGE * stage_bytes(lossy) + NB + 256;
-    }
-    // bytes a full stage (E, H, ce[, ca]) and an E-only stage deliver
+    static constexpr int NB = 3 * HB;  // H^{n+1/2}(p) on the tile + halo, H-box layout
     __host__ __device__ static constexpr uint32_t tx_full(bool lossy) {
         return 3u * (EW * EH + HW * HH + TK * TJ * (lossy ? 2 : 1)) * sizeof(T);
     }
@@ -126,44 +142,71 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+template <typename T, int V>
+__device__ __forceinline__ void ld_vec(const T *p, T (&out)[V]) {
+    using VT = typename VecT<T>::type;
+    const VT v = *reinterpret_cast<const VT *>(p);
+    const T *q = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int e = 0; e < V; ++e) out[e] = q[e];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
+    using VT = typename VecT<T>::type;
+    VT v;
+    T *q = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int e = 0; e < V; ++e) q[e] = in[e];
+    *reinterpret_cast<VT *>(p) = v;
+}
+
+struct InteriorBox {
+    int lo[3], hi[3];  // H box B = [lo, hi); E box B' = [lo+1, hi)
+    int j0base, k0base, ntk, chunk;
+    // dynamic shared memory layout (bytes)
+    int stage_bytes, new_off, bar_off;
+};
+
 // ---------------------------------------------------------------- the kernel
-template <typename T, bool LOSSY>
+template <typename T, bool LOSSY, int NSTAGE>
 __global__ void __launch_bounds__(NTHREADS, 2)
-    k_step_fused(const __grid_constant__ FusedMaps maps, const YeeArgs<T> a,
-                 const SourceList src, const PlaneList planes, int ntk, int chunk) {
-    using L = FusedTile<T>;
-    constexpr int TK = L::TK, TJ = L::TJ, HP = L::HP, NTY = L::NTY, RPT = L::RPT;
-    constexpr int EW = L::EW, EH = L::EH, HW = L::HW, NW = L::NW;
+    k_interior(const __grid_constant__ FusedMaps maps, const YeeArgs<T> a,
+               const __grid_constant__ InteriorBox bx, const __grid_constant__ SourceList src) {
+    using L = Tile<T>;
+    constexpr int V = L::V, TK = L::TK, TJ = L::TJ, EW = L::EW, HW = L::HW;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    constexpr int SB = L::stage_bytes(LOSSY);
-    T *sNew = reinterpret_cast<T *>(smem + NSTAGE * SB);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + NSTAGE * SB + L::NB);
+    const int SB = bx.stage_bytes;
+    T *sNew = reinterpret_cast<T *>(smem + bx.new_off);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + bx.bar_off);
 
-    const int nx = a.nx, ny = a.ny, nz = a.nz, npml = a.npml;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int tile = blockIdx.x;
-    const int k0 = (tile % ntk) * TK;
-    const int j0 = (tile / ntk) * TJ;
-    const int i0 = blockIdx.y * chunk;
-    const int i1 = min(nx, i0 + chunk);
-    const int pfirst = (i0 > 0) ? i0 - 1 : 0;  // first plane whose H^{n+1/2} is computed
-    const int plast = i1;                      // last plane loaded (E only when == i1)
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * TK + tx;
+    const int k0 = bx.k0base + (tile % bx.ntk) * TK;
+    const int j0 = bx.j0base + (tile / bx.ntk) * TJ;
+    const int i0 = bx.lo[0] + blockIdx.y * bx.chunk;
+    const int i1 = min(bx.hi[0], i0 + bx.chunk);
+    const int pfirst = (i0 > bx.lo[0]) ? i0 - 1 : i0;  // pre-plane recomputes H(i0-1)
+    const int plast = i1;                               // E only
+    const int tid = threadIdx.x;
+    const bool cell_thr = tid < NCELLTHR;
+    const int g = tid % L::G, r = tid / L::G;  // cell threads: vector group, row
 
-    auto stage_ptr = [&](int s) { return smem + s * SB; };
-    auto sE = [&](int s, int c) { return reinterpret_cast<T *>(stage_ptr(s) + c * L::EB); };
+    auto sE = [&](int s, int c) {
+        return reinterpret_cast<T *>(smem + s * SB + c * L::EB);
+    };
     auto sH = [&](int s, int c) {
-        return reinterpret_cast<T *>(stage_ptr(s) + 3 * L::EB + c * L::HB);
+        return reinterpret_cast<T *>(smem + s * SB + 3 * L::EB + c * L::HB);
     };
     auto sC = [&](int s, int c) {
-        return reinterpret_cast<T *>(stage_ptr(s) + 3 * L::EB + 3 * L::HB + c * L::CB);
+        return reinterpret_cast<T *>(smem + s * SB + 3 * L::EB + 3 * L::HB + c * L::CB);
     };
     auto sA = [&](int s, int c) {
-        return reinterpret_cast<T *>(stage_ptr(s) + 3 * L::EB + 3 * L::HB + (3 + c) * L::CB);
+        return reinterpret_cast<T *>(smem + s * SB + 3 * L::EB + 3 * L::HB + (3 + c) * L::CB);
     };
-
+    auto sN = [&](int c) { return reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sNew) + c * L::HB); };
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; ++s) mbar_init(&bar[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -171,32 +214,49 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     }
     __syncthreads();
 
-    // producer: issue the loads of plane p into its stage
     auto issue = [&](int p) {
         const int s = (p - pfirst) % NSTAGE;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         if (p < plast) {
             mbar_expect_tx(&bar[s], L::tx_full(LOSSY));
             for (int c = 0; c < 3; ++c) {
-                tma_load_3d(sE(s, c), &maps.E[c], &bar[s], k0 - HP, j0 - 1, p);
-                tma_load_3d(sH(s, c), &maps.H[c], &bar[s], k0 - HP, j0 - 1, p);
+                tma_load_3d(sE(s, c), &maps.E[c], &bar[s], k0 - V, j0 - 1, p);
+                tma_load_3d(sH(s, c), &maps.H[c], &bar[s], k0 - V, j0 - 1, p);
                 tma_load_3d(sC(s, c), &maps.C[c], &bar[s], k0, j0, p);
                 if (LOSSY) tma_load_3d(sA(s, c), &maps.A[c], &bar[s], k0, j0, p);
             }
         } else {
             mbar_expect_tx(&bar[s], L::tx_eonly());
-            for (int c = 0; c < 3; ++c) tma_load_3d(sE(s, c), &maps.E[c], &bar[s], k0 - HP, j0 - 1, p);
+            for (int c = 0; c < 3; ++c)
+                tma_load_3d(sE(s, c), &maps.E[c], &bar[s], k0 - V, j0 - 1, p);
         }
     };
     if (tid == 0)
         for (int p = pfirst; p <= plast && p < pfirst + NSTAGE; ++p) issue(p);
 
-    const T dtm = a.dtm, dtm_dl = a.dtm_dl, inv_dl = a.inv_dl;
-    const int64_t sx = (int64_t)ny * nz, sy = nz;
-
-    T carry_hy[RPT], carry_hz[RPT];
+    const T dtm_dl = a.dtm_dl, inv_dl = a.inv_dl;
+    const int64_t sx = (int64_t)ny * nz;
+    // cell thread geometry
+    const int j = j0 + r;
+    const int kb = k0 + V * g;
+    const bool rowH = j >= bx.lo[1] && j < bx.hi[1];
+    const bool rowE = j >= bx.lo[1] + 1 && j < bx.hi[1];
+    bool kH[V], kE[V];
+    bool allH = rowH, allE = rowE;
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) carry_hy[r] = carry_hz[r] = T(0);
+    for (int v = 0; v < V; ++v) {
+        kH[v] = (kb + v) >= bx.lo[2] && (kb + v) < bx.hi[2];
+        kE[v] = (kb + v) >= bx.lo[2] + 1 && (kb + v) < bx.hi[2];
+        allH = allH && kH[v];
+        allE = allE && kE[v];
+    }
+    const int eo = (r + 1) * EW + V + V * g;  // own cells in the E box
+    const int ho = (r + 1) * HW + V + V * g;  // own cells in the H / new-H box
+    const int co = r * TK + V * g;            // own cells in the coefficient box
+
+    T hyc[V], hzc[V];  // H^{n+1/2}(p-1) at own cells
+#pragma unroll
+    for (int v = 0; v < V; ++v) hyc[v] = hzc[v] = T(0);
 
     bool ok = true;
     for (int p = pfirst; p < plast; ++p) {
@@ -207,149 +267,179 @@ __global__ void __launch_bounds__(NTHREADS, 2)
             ok = false;
             break;
         }
-        const bool real_plane = (p >= i0);
-        const T *E0[3] = {sE(s, 0), sE(s, 1), sE(s, 2)};
-        const T *E1[3] = {sE(s1, 0), sE(s1, 1), sE(s1, 2)};
-        const T *H0[3] = {sH(s, 0), sH(s, 1), sH(s, 2)};
-        // smem index of grid cell (j, k) in the E / H regions
-        auto ei = [&](int j, int k) { return (j - j0 + 1) * EW + (k - k0 + HP); };
-        auto hi = [&](int j, int k) { return (j - j0 + 1) * HW + (k - k0 + HP); };
-        auto ni = [&](int j, int k) { return (j - j0 + 1) * NW + (k - k0 + 1); };
-
-        // H^{n+1/2}(p) at (j, k); returns the three components
-        auto h_at = [&](int j, int k, bool own, T &hx, T &hy, T &hz) {
-            const bool interior = is_interior(p, j, k, nx, ny, nz, npml);
-            const int e = ei(j, k);
-            const T ex0 = E0[0][e], ey0 = E0[1][e], ez0 = E0[2][e];
-            DE<T> d;
-            if (interior) {
-                d.zy = E0[2][e + EW] - ez0;
-                d.yz = E0[1][e + 1] - ey0;
-                d.xz = E0[0][e + 1] - ex0;
-                d.zx = E1[2][e] - ez0;
-                d.yx = E1[1][e] - ey0;
-                d.xy = E0[0][e + EW] - ex0;
-            } else {
-                d.zy = (j < ny - 1) ? (E0[2][e + EW] - ez0) : T(0);
-                d.yz = (k < nz - 1) ? (E0[1][e + 1] - ey0) : T(0);
-                d.xz = (k < nz - 1) ? (E0[0][e + 1] - ex0) : T(0);
-                d.zx = (p < nx - 1) ? (E1[2][e] - ez0) : T(0);
-                d.yx = (p < nx - 1) ? (E1[1][e] - ey0) : T(0);
-                d.xy = (j < ny - 1) ? (E0[0][e + EW] - ex0) : T(0);
+        const bool storeH = p >= i0;
+        const bool doE = p >= i0 && p >= bx.lo[0] + 1;
+        const T *E0x = sE(s, 0), *E0y = sE(s, 1), *E0z = sE(s, 2);
+        const T *E1y = sE(s1, 1), *E1z = sE(s1, 2);
+        T ex0[V], ey0[V], ez0[V], hx[V], hy[V], hz[V];
+        if (cell_thr) {
+            T ezj[V], exj[V], ez1[V], ey1[V];
+            ld_vec<T, V>(E0x + eo, ex0);
+            ld_vec<T, V>(E0y + eo, ey0);
+            ld_vec<T, V>(E0z + eo, ez0);
+            ld_vec<T, V>(E0z + eo + EW, ezj);
+            ld_vec<T, V>(E0x + eo + EW, exj);
+            ld_vec<T, V>(E1z + eo, ez1);
+            ld_vec<T, V>(E1y + eo, ey1);
+            ld_vec<T, V>(sH(s, 0) + ho, hx);
+            ld_vec<T, V>(sH(s, 1) + ho, hy);
+            ld_vec<T, V>(sH(s, 2) + ho, hz);
+            // k+1 of the last cell: first cell of the next thread in the row, or
+            // the tile's halo column for the last thread
+            T eyn = __shfl_down_sync(0xffffffffu, ey0[0], 1);
+            T exn = __shfl_down_sync(0xffffffffu, ex0[0], 1);
+            if (g == L::G - 1) {
+                eyn = E0y[eo + V];
+                exn = E0x[eo + V];
             }
-            const int h = hi(j, k);
-            hx = H0[0][h];
-            hy = H0[1][h];
-            hz = H0[2][h];
-            if (own && real_plane)
-                h_cell<T, true>(interior, p, j, k, nx, ny, nz, npml, dtm, dtm_dl, d, a.cph,
-                                a.psi_h, a.psi_h_next, hx, hy, hz);
-            else
-                h_cell<T, false>(interior, p, j, k, nx, ny, nz, npml, dtm, dtm_dl, d, a.cph,
-                                 a.psi_h, a.psi_h_next, hx, hy, hz);
-        };
-
-        T own_h[RPT][3];
-        const int k = k0 + tx;
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int j = j0 + ty * RPT + r;
-            if (k < nz && j < ny) {
-                h_at(j, k, true, own_h[r][0], own_h[r][1], own_h[r][2]);
-                const int n = ni(j, k);
-                sNew[0 * L::NW * L::NH + n] = own_h[r][0];
-                sNew[1 * L::NW * L::NH + n] = own_h[r][1];
-                sNew[2 * L::NW * L::NH + n] = own_h[r][2];
+            for (int v = 0; v < V; ++v) {
+                const T eyk = (v < V - 1) ? ey0[v + 1] : eyn;
+                const T exk = (v < V - 1) ? ex0[v + 1] : exn;
+                const T d_zy = ezj[v] - ez0[v], d_yz = eyk - ey0[v], d_xz = exk - ex0[v];
+                const T d_zx = ez1[v] - ez0[v], d_yx = ey1[v] - ey0[v], d_xy = exj[v] - ex0[v];
+                hx[v] = hx[v] - dtm_dl * (d_zy - d_yz);
+                hy[v] = hy[v] - dtm_dl * (d_xz - d_zx);
+                hz[v] = hz[v] - dtm_dl * (d_yx - d_xy);
             }
-        }
-        if (real_plane) {
-            // halo row j0-1 (k in tile) and halo column k0-1 (j in tile)
-            if (tid < TK) {
-                const int kh = k0 + tid, jh = j0 - 1;
-                if (jh >= 0 && kh < nz) {
-                    T hx, hy, hz;
-                    h_at(jh, kh, false, hx, hy, hz);
-                    const int n = ni(jh, kh);
-                    sNew[0 * L::NW * L::NH + n] = hx;
-                    sNew[1 * L::NW * L::NH + n] = hy;
-                    sNew[2 * L::NW * L::NH + n] = hz;
+            st_vec<T, V>(sN(0) + ho, hx);
+            st_vec<T, V>(sN(1) + ho, hy);
+            st_vec<T, V>(sN(2) + ho, hz);
+            if (storeH && rowH) {
+                const int64_t gi = (int64_t)p * sx + (int64_t)j * nz + kb;
+                if (allH) {
+                    st_vec<T, V>(a.H_next[0] + gi, hx);
+                    st_vec<T, V>(a.H_next[1] + gi, hy);
+                    st_vec<T, V>(a.H_next[2] + gi, hz);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        if (kH[v]) {
+                            a.H_next[0][gi + v] = hx[v];
+                            a.H_next[1][gi + v] = hy[v];
+                            a.H_next[2][gi + v] = hz[v];
+                        }
                 }
-            } else if (tid < TK + TJ) {
-                const int jh = j0 + (tid - TK), kh = k0 - 1;
-                if (kh >= 0 && jh < ny) {
-                    T hx, hy, hz;
-                    h_at(jh, kh, false, hx, hy, hz);
-                    const int n = ni(jh, kh);
-                    sNew[0 * L::NW * L::NH + n] = hx;
-                    sNew[1 * L::NW * L::NH + n] = hy;
-                    sNew[2 * L::NW * L::NH + n] = hz;
+            }
+        } else if (doE) {
+            // halo warp: H^{n+1/2} on row j0-1 (lanes 0..15) and column k0-1 (lanes 16..23)
+            const int lane = tid - NCELLTHR;
+            if (lane < L::G) {
+                if (j0 - 1 >= bx.lo[1]) {
+                    const int e = V + V * lane, h = V + V * lane;  // E box row 0, H box row 0
+                    T a0[V], a1[V], a2[V], zj[V], xj[V], z1[V], y1[V], qx[V], qy[V], qz[V];
+                    ld_vec<T, V>(E0x + e, a0);
+                    ld_vec<T, V>(E0y + e, a1);
+                    ld_vec<T, V>(E0z + e, a2);
+                    ld_vec<T, V>(E0z + e + EW, zj);
+                    ld_vec<T, V>(E0x + e + EW, xj);
+                    ld_vec<T, V>(E1z + e, z1);
+                    ld_vec<T, V>(E1y + e, y1);
+                    ld_vec<T, V>(sH(s, 0) + h, qx);
+                    ld_vec<T, V>(sH(s, 1) + h, qy);
+                    ld_vec<T, V>(sH(s, 2) + h, qz);
+                    const T yn = E0y[e + V], xn = E0x[e + V];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const T yk = (v < V - 1) ? a1[v + 1] : yn;
+                        const T xk = (v < V - 1) ? a0[v + 1] : xn;
+                        const T d_zy = zj[v] - a2[v], d_yz = yk - a1[v], d_xz = xk - a0[v];
+                        const T d_zx = z1[v] - a2[v], d_yx = y1[v] - a1[v], d_xy = xj[v] - a0[v];
+                        qx[v] = qx[v] - dtm_dl * (d_zy - d_yz);
+                        qy[v] = qy[v] - dtm_dl * (d_xz - d_zx);
+                        qz[v] = qz[v] - dtm_dl * (d_yx - d_xy);
+                    }
+                    st_vec<T, V>(sN(0) + h, qx);
+                    st_vec<T, V>(sN(1) + h, qy);
+                    st_vec<T, V>(sN(2) + h, qz);
+                }
+            } else if (lane < L::G + TJ) {
+                const int rr = lane - L::G;
+                if (k0 - 1 >= bx.lo[2] && j0 + rr < ny) {
+                    const int e = (rr + 1) * EW + V - 1, h = (rr + 1) * HW + V - 1;
+                    const T x0 = E0x[e], y0 = E0y[e], z0 = E0z[e];
+                    const T d_zy = E0z[e + EW] - z0, d_yz = E0y[e + 1] - y0;
+                    const T d_xz = E0x[e + 1] - x0, d_zx = E1z[e] - z0;
+                    const T d_yx = E1y[e] - y0, d_xy = E0x[e + EW] - x0;
+                    sN(0)[h] = sH(s, 0)[h] - dtm_dl * (d_zy - d_yz);
+                    sN(1)[h] = sH(s, 1)[h] - dtm_dl * (d_xz - d_zx);
+                    sN(2)[h] = sH(s, 2)[h] - dtm_dl * (d_yx - d_xy);
                 }
             }
         }
         __syncthreads();
 
-        if (real_plane) {
-            const T *NXp = sNew, *NYp = sNew + L::NW * L::NH, *NZp = sNew + 2 * L::NW * L::NH;
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int j = j0 + ty * RPT + r;
-                if (k >= nz || j >= ny) continue;
-                const bool interior = is_interior(p, j, k, nx, ny, nz, npml);
-                const int n = ni(j, k);
-                const T hx0 = own_h[r][0], hy0 = own_h[r][1], hz0 = own_h[r][2];
-                DH<T> d;
-                if (interior) {
-                    d.zy = hz0 - NZp[n - NW];
-                    d.yz = hy0 - NYp[n - 1];
-                    d.xz = hx0 - NXp[n - 1];
-                    d.zx = hz0 - carry_hz[r];
-                    d.yx = hy0 - carry_hy[r];
-                    d.xy = hx0 - NXp[n - NW];
-                } else {
-                    d.zy = (j > 0) ? (hz0 - NZp[n - NW]) : T(0);
-                    d.yz = (k > 0) ? (hy0 - NYp[n - 1]) : T(0);
-                    d.xz = (k > 0) ? (hx0 - NXp[n - 1]) : T(0);
-                    d.zx = (p > 0) ? (hz0 - carry_hz[r]) : T(0);
-                    d.yx = (p > 0) ? (hy0 - carry_hy[r]) : T(0);
-                    d.xy = (j > 0) ? (hx0 - NXp[n - NW]) : T(0);
-                }
-                const int c = (j - j0) * TK + (k - k0);
-                const int e = ei(j, k);
-                const T cex = sC(s, 0)[c], cey = sC(s, 1)[c], cez = sC(s, 2)[c];
-                T cax = T(1), cay = T(1), caz = T(1);
-                if (LOSSY) {
-                    cax = sA(s, 0)[c];
-                    cay = sA(s, 1)[c];
-                    caz = sA(s, 2)[c];
-                }
-                T ex = E0[0][e], ey = E0[1][e], ez = E0[2][e];
-                if (src.n) ex = apply_sources<T>(src, p, j, k, ex, cex);
-                e_cell<T, LOSSY>(interior, p, j, k, nx, ny, nz, npml, inv_dl, d, a.cpe, a.psi_e,
-                                 cax, cay, caz, cex, cey, cez, ex, ey, ez);
-                const int64_t idx = (int64_t)p * sx + (int64_t)j * sy + k;
-                a.H_next[0][idx] = hx0;
-                a.H_next[1][idx] = hy0;
-                a.H_next[2][idx] = hz0;
-                a.E_next[0][idx] = ex;
-                a.E_next[1][idx] = ey;
-                a.E_next[2][idx] = ez;
-                if (planes.n) {
-                    const double v[6] = {(double)ex, (double)ey, (double)ez,
-                                         (double)hx0, (double)hy0, (double)hz0};
-                    plane_dft_cell(planes, p, j, k, nx, ny, nz, v);
-                }
+        T hyk0 = T(0), hxk0 = T(0);
+        if (doE && cell_thr) {
+            // k-1 of the first cell: last cell of the previous thread in the row,
+            // or the tile's halo column for the first thread
+            hyk0 = __shfl_up_sync(0xffffffffu, hy[V - 1], 1);
+            hxk0 = __shfl_up_sync(0xffffffffu, hx[V - 1], 1);
+            if (g == 0) {
+                hyk0 = sN(1)[ho - 1];
+                hxk0 = sN(0)[ho - 1];
             }
         }
+        if (doE && cell_thr && rowE) {
+            T hzj[V], hxj[V], cex[V], cey[V], cez[V];
+            ld_vec<T, V>(sN(2) + ho - HW, hzj);
+            ld_vec<T, V>(sN(0) + ho - HW, hxj);
+            ld_vec<T, V>(sC(s, 0) + co, cex);
+            ld_vec<T, V>(sC(s, 1) + co, cey);
+            ld_vec<T, V>(sC(s, 2) + co, cez);
+            T cax[V], cay[V], caz[V];
+            if (LOSSY) {
+                ld_vec<T, V>(sA(s, 0) + co, cax);
+                ld_vec<T, V>(sA(s, 1) + co, cay);
+                ld_vec<T, V>(sA(s, 2) + co, caz);
+            }
+            // injections: a uniform plane/tile test first, then per cell
+            bool src_here = false;
+            for (int q = 0; q < src.n; ++q) {
+                const fdtd_source &sq = src.s[q];
+                src_here |= p >= sq.i0 && p < sq.i1 && j >= sq.j0 && j < sq.j1 &&
+                            sq.z >= kb && sq.z < kb + V;
+            }
+            if (src_here) {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            carry_hy[r] = own_h[r][1];
-            carry_hz[r] = own_h[r][2];
+                for (int v = 0; v < V; ++v) ex0[v] = apply_sources<T>(src, p, j, kb + v, ex0[v], cex[v]);
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const T hyk = v ? hy[v - 1] : hyk0;
+                const T hxk = v ? hx[v - 1] : hxk0;
+                const T d_zy = hz[v] - hzj[v], d_yz = hy[v] - hyk, d_xz = hx[v] - hxk;
+                const T d_zx = hz[v] - hzc[v], d_yx = hy[v] - hyc[v], d_xy = hx[v] - hxj[v];
+                ex0[v] = (LOSSY ? cax[v] * ex0[v] : ex0[v]) + cex[v] * inv_dl * (d_zy - d_yz);
+                ey0[v] = (LOSSY ? cay[v] * ey0[v] : ey0[v]) + cey[v] * inv_dl * (d_xz - d_zx);
+                ez0[v] = (LOSSY ? caz[v] * ez0[v] : ez0[v]) + cez[v] * inv_dl * (d_yx - d_xy);
+            }
+            const int64_t gi = (int64_t)p * sx + (int64_t)j * nz + kb;
+            if (allE) {
+                st_vec<T, V>(a.E_next[0] + gi, ex0);
+                st_vec<T, V>(a.E_next[1] + gi, ey0);
+                st_vec<T, V>(a.E_next[2] + gi, ez0);
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v)
+                    if (kE[v]) {
+                        a.E_next[0][gi + v] = ex0[v];
+                        a.E_next[1][gi + v] = ey0[v];
+                        a.E_next[2][gi + v] = ez0[v];
+                    }
+            }
         }
-        __syncthreads();  // stage s and sNew are free
+        if (cell_thr) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                hyc[v] = hy[v];
+                hzc[v] = hz[v];
+            }
+        }
+        __syncthreads();  // stage s and the new-H plane are free
         if (tid == 0 && p + NSTAGE <= plast) issue(p + NSTAGE);
     }
     if (!ok) {
-        // drain: wait (bounded) for every stage that may still have copies in flight
         __syncthreads();
         if (tid == 0) {
             for (int p = pfirst; p <= plast; ++p) {
@@ -430,17 +520,27 @@ bool make_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int el
     return true;
 }
 
-// Chunks along i: enough CTAs to fill ~2 per SM over whole waves, chunk >= 16 planes.
-int choose_chunks(int tiles, int nx, int sms) {
-    const int slots = 2 * sms;
+// Pipeline depth of the interior kernel: 4 stages (2 CTAs per SM) by default;
+// FDTD_B200_NSTAGE=3 selects 3 stages (3 CTAs per SM) as a tuning knob.
+int stage_count() {
+    static int n = [] {
+        const char *v = getenv("FDTD_B200_NSTAGE");
+        return (v && atoi(v) == 3) ? 3 : NSTAGE_DEFAULT;
+    }();
+    return n;
+}
+
+// Chunks along i: whole waves of resident CTAs, chunks of at least 16 planes.
+int choose_chunks(int tiles, int nplanes, int sms) {
+    const int slots = (stage_count() == 3 ? 3 : 2) * sms;
     int best = 1;
     double best_score = -1.0;
-    for (int c = 1; c <= 32; ++c) {
-        const int len = (nx + c - 1) / c;
+    for (int c = 1; c <= 64; ++c) {
+        const int len = (nplanes + c - 1) / c;
         if (len < 16 && c > 1) break;
         const double waves = (double)tiles * c / slots;
-        const double fill = waves / ceil(waves);
-        const double score = fill * (1.0 - 1.5 / (len + 1.5));
+        const double fill = waves / std::ceil(waves);
+        const double score = fill * (1.0 - 1.0 / (len + 1.0));
         if (score > best_score + 1e-9) {
             best_score = score;
             best = c;
@@ -449,55 +549,105 @@ int choose_chunks(int tiles, int nx, int sms) {
     return best;
 }
 
-}  // namespace
-
 template <typename T>
-cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const PlaneList &pl,
-                              cudaStream_t st) {
-    using L = FusedTile<T>;
+bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
+    using L = Tile<T>;
     const int elem = (int)sizeof(T);
-    // TMA needs 16-byte aligned row strides and base addresses.
-    if (((int64_t)a.nz * elem) % 16 != 0) return cudaErrorNotSupported;
-    for (int c = 0; c < 3; ++c) {
-        const void *ptrs[5] = {a.E[c], a.H[c], a.ce[c], a.E_next[c], a.H_next[c]};
-        for (const void *q : ptrs)
-            if (reinterpret_cast<uintptr_t>(q) % 16 != 0) return cudaErrorNotSupported;
-        if (a.lossy && reinterpret_cast<uintptr_t>(a.ca[c]) % 16 != 0) return cudaErrorNotSupported;
-    }
-    FusedMaps maps;
     memset(&maps, 0, sizeof(maps));
     for (int c = 0; c < 3; ++c) {
         if (!make_map(&maps.E[c], a.E[c], a.nx, a.ny, a.nz, elem, L::EW, L::EH) ||
             !make_map(&maps.H[c], a.H[c], a.nx, a.ny, a.nz, elem, L::HW, L::HH) ||
             !make_map(&maps.C[c], a.ce[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
-            return cudaErrorNotSupported;
+            return false;
         if (a.lossy && !make_map(&maps.A[c], a.ca[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
-            return cudaErrorNotSupported;
+            return false;
     }
+    return true;
+}
+
+template <typename T>
+cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const ShellBox &hb,
+                            const SourceList &src, cudaStream_t st) {
+    using L = Tile<T>;
+    InteriorBox bx;
+    for (int d = 0; d < 3; ++d) {
+        bx.lo[d] = hb.lo[d];
+        bx.hi[d] = hb.hi[d];
+    }
+    bx.k0base = (hb.lo[2] / L::V) * L::V;  // TMA x coordinates stay 16-byte aligned
+    bx.j0base = hb.lo[1];
+    bx.ntk = (hb.hi[2] - bx.k0base + L::TK - 1) / L::TK;
+    const int ntj = (hb.hi[1] - bx.j0base + L::TJ - 1) / L::TJ;
+    const int tiles = bx.ntk * ntj;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ntk = (a.nz + L::TK - 1) / L::TK;
-    const int ntj = (a.ny + L::TJ - 1) / L::TJ;
-    const int tiles = ntk * ntj;
-    const int nchunk = choose_chunks(tiles, a.nx, sms);
-    const int chunk = (a.nx + nchunk - 1) / nchunk;
-    dim3 grid(tiles, (a.nx + chunk - 1) / chunk, 1);
-    dim3 block(L::TK, L::NTY, 1);
-    const size_t smem = L::smem_bytes(a.lossy != 0);
-    cudaError_t e;
+    const int nplanes = hb.hi[0] - hb.lo[0];
+    const int nchunk = choose_chunks(tiles, nplanes, sms);
+    bx.chunk = (nplanes + nchunk - 1) / nchunk;
+    dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
+    bx.stage_bytes = L::stage_bytes(a.lossy != 0);
+    const int nstage = stage_count();
+    bx.new_off = nstage * bx.stage_bytes;
+    bx.bar_off = bx.new_off + L::NB;
+    const size_t smem = bx.bar_off + 64 + 128;
+    cudaError_t e = cudaSuccess;
+#define FDTD_LAUNCH_INTERIOR(LS, NS)                                                           \
+    do {                                                                                       \
+        e = cudaFuncSetAttribute(k_interior<T, LS, NS>,                                        \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+        if (e != cudaSuccess) return e;                                                        \
+        k_interior<T, LS, NS><<<grid, NTHREADS, smem, st>>>(maps, a, bx, src);                 \
+    } while (0)
     if (a.lossy) {
-        e = cudaFuncSetAttribute(k_step_fused<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        k_step_fused<T, true><<<grid, block, smem, st>>>(maps, a, src, pl, ntk, chunk);
+        if (nstage == 3) FDTD_LAUNCH_INTERIOR(true, 3);
+        else FDTD_LAUNCH_INTERIOR(true, 4);
     } else {
-        e = cudaFuncSetAttribute(k_step_fused<T, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_step_fused<T, false><<<grid, block, smem, st>>>(maps, a, src, pl, ntk, chunk);
+        if (nstage == 3) FDTD_LAUNCH_INTERIOR(false, 3);
+        else FDTD_LAUNCH_INTERIOR(false, 4);
     }
+#undef FDTD_LAUNCH_INTERIOR
     return cudaGetLastError();
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const PlaneList &pl,
+                              cudaStream_t st) {
+    const int elem = (int)sizeof(T);
+    const int n[3] = {a.nx, a.ny, a.nz};
+    // interior H box [npml, N-npml)^3; the fused kernel needs npml >= 1, a non
+    // empty E box and TMA-compatible (16-byte) strides and base addresses
+    bool use_interior = a.npml >= 1 && ((int64_t)a.nz * elem) % 16 == 0;
+    for (int d = 0; d < 3; ++d) use_interior = use_interior && n[d] - 2 * a.npml >= 2;
+    for (int c = 0; c < 3 && use_interior; ++c) {
+        const void *ptrs[5] = {a.E[c], a.H[c], a.ce[c], a.E_next[c], a.H_next[c]};
+        for (const void *q : ptrs)
+            if (reinterpret_cast<uintptr_t>(q) % 16 != 0) use_interior = false;
+        if (a.lossy && reinterpret_cast<uintptr_t>(a.ca[c]) % 16 != 0) use_interior = false;
+    }
+    FusedMaps maps;
+    if (use_interior && !build_maps<T>(a, maps)) use_interior = false;
+    ShellBox hbox, ebox;
+    for (int d = 0; d < 3; ++d) {
+        hbox.lo[d] = use_interior ? a.npml : 0;
+        hbox.hi[d] = use_interior ? n[d] - a.npml : 0;
+        ebox.lo[d] = use_interior ? a.npml + 1 : 0;
+        ebox.hi[d] = use_interior ? n[d] - a.npml : 0;
+    }
+    cudaError_t e = launch_shell_H<T>(a, hbox, st);
+    if (e != cudaSuccess) return e;
+    if (use_interior) {
+        e = launch_interior<T>(a, maps, hbox, src, st);
+        if (e != cudaSuccess) return e;
+        // plane DFTs of the cells the interior kernel updated
+        if (pl.n) {
+            e = launch_plane_dft_box<T>(a, ebox, pl, st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return launch_shell_E<T>(a, ebox, src, pl, st);
 }
 
 template cudaError_t launch_step_fused<float>(const YeeArgs<float> &, const SourceList &,

@@ -25,6 +25,23 @@ struct YeeArgs {
     T *psi_e[6];
 };
 
+// Box [lo, hi) per axis; lo == hi == 0 on every axis means "no box".
+struct ShellBox {
+    int lo[3], hi[3];
+};
+
+template <typename T>
+cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t st);
+template <typename T>
+cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceList &src,
+                           const PlaneList &pl, cudaStream_t st);
+
+// Plane-DFT accumulation for the monitored planes' cells inside box b (read
+// back from E_next / H_next after the interior update).
+template <typename T>
+cudaError_t launch_plane_dft_box(const YeeArgs<T> &a, const ShellBox &b, const PlaneList &pl,
+                                 cudaStream_t st);
+
 template <typename T>
 cudaError_t launch_update_H(const YeeArgs<T> &a, cudaStream_t st);
 template <typename T>
@@ -33,8 +50,9 @@ cudaError_t launch_update_E(const YeeArgs<T> &a, const SourceList &src, const Pl
 template <typename T>
 cudaError_t launch_add_source(int nx, int ny, int nz, const fdtd_source &s, T *Ex,
                               const T *ce_x, cudaStream_t st);
-// Fused single-pass step; returns cudaErrorNotSupported when the shape or the
-// alignment does not admit the fused schedule (the caller then runs H and E).
+// Fused step: shell H, interior single-pass kernel, shell E.  Reads E/H/psi,
+// writes E_next/H_next (psi in place).  Falls back to the shell kernels over
+// the whole grid when the interior kernel's TMA alignment does not hold.
 template <typename T>
 cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const PlaneList &pl,
                               cudaStream_t st);

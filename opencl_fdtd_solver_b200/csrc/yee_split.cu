@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(SPLIT_TK *SPLIT_TJ)
     a.E[0][idx] = ex;
     a.E[1][idx] = ey;
     a.E[2][idx] = ez;
-    if (planes.n) {
+    if (planes.n && plane_any_hit(planes, i, j, k)) {
         const double v[6] = {(double)ex, (double)ey, (double)ez,
                              (double)hx0, (double)hy0, (double)hz0};
         plane_dft_cell(planes, i, j, k, nx, ny, nz, v);

@@ -149,8 +149,8 @@ class CUDAFDTD(SourceMonitorMixin):
 
     @staticmethod
     def device_footprint_bytes(shape, npml, dtype=np.float32, *, lossy=False, fused=True):
-        """Bytes this engine actually allocates: fields (twice when fused), ``ce``
-        (and ``ca`` when lossy), ψ_E, ψ_H (twice when fused)."""
+        """Bytes this engine actually allocates: fields (twice when fused, the step
+        reads one set and writes the other), ``ce`` (and ``ca`` when lossy), ψ stripes."""
         nx, ny, nz = shape
         item = np.dtype(dtype).itemsize
         cells = nx * ny * nz
@@ -158,7 +158,7 @@ class CUDAFDTD(SourceMonitorMixin):
         psi_one = 0
         if npml > 0:
             psi_one = 2 * (2 * npml * ny * nz + nx * 2 * npml * nz + nx * ny * 2 * npml)
-        return (arrays * cells + psi_one * (3 if fused else 2)) * item
+        return (arrays * cells + psi_one * 2) * item
 
     @classmethod
     def device_memory_budget_bytes(cls, device):
@@ -226,7 +226,6 @@ class CUDAFDTD(SourceMonitorMixin):
         order = (sy, sz, sx, sz, sx, sy)  # Hx_y, Hx_z, Hy_x, Hy_z, Hz_x, Hz_y / E likewise
         with torch.cuda.stream(self.queue):
             self._psi_h = [mk(s) for s in order]
-            self._psi_hn = [mk(s) for s in order] if self._fused_enabled else None
             self._psi_e = [mk(s) for s in order]
 
     def _build_structs(self):
@@ -264,8 +263,6 @@ class CUDAFDTD(SourceMonitorMixin):
         for q in range(6):
             cp.psi_h[q] = self._psi_h[q].data_ptr()
             cp.psi_e[q] = self._psi_e[q].data_ptr()
-            if self._psi_hn is not None:
-                cp.psi_h_next[q] = self._psi_hn[q].data_ptr()
         self._cpml = cp
         self._grid.lossy = 1 if self.lossy else 0
 
@@ -413,7 +410,6 @@ class CUDAFDTD(SourceMonitorMixin):
     def _swap(self):
         self._E, self._En = self._En, self._E
         self._H, self._Hn = self._Hn, self._H
-        self._psi_h, self._psi_hn = self._psi_hn, self._psi_h
         self._parity ^= 1
         self._refresh_structs()
 

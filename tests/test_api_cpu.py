@@ -155,9 +155,9 @@ def test_memory_estimate_matches_reference_formula():
     reserve = Dev.global_mem_size - budget
     assert reserve >= CUDAFDTD.MEMORY_HEADROOM_BYTES
     assert reserve >= int(Dev.global_mem_size * CUDAFDTD.MEMORY_HEADROOM_FRACTION)
-    # the engine's own footprint: 12 field arrays + 3 ce + ψ (ψ_H twice) when fused
+    # the engine's own footprint: 12 field arrays + 3 ce + 12 ψ stripes when fused
     fp = CUDAFDTD.device_footprint_bytes((512, 512, 512), 16, np.float32)
-    assert fp == (15 * 512**3 + 3 * 2 * 3 * 2 * 16 * 512 * 512) * 4
+    assert fp == (15 * 512**3 + 2 * 3 * 2 * 2 * 16 * 512 * 512) * 4
 
 
 def test_memory_error_before_allocation():
