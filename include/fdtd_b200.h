@@ -161,6 +161,20 @@ int fdtd_dft_rel_change(const double *cur, const double *prev, int32_t n_face,
                         int32_t nfreq, int32_t fi, double *scratch, double *out2,
                         void *stream);
 
+/* The same relative change with no device memory supplied by the caller, for
+ * callers that must not allocate at run time: drivers that keep the device
+ * busy asynchronously (cudaMalloc/cudaFree may synchronise the device and
+ * would stall the time-step stream) and hosts whose device memory is a fixed
+ * pool set up at start-up.  Its partial sums live in a 16 KiB array inside
+ * the library (held on every GPU that loads it until the process exits), so
+ * n_face is limited to FDTD_NOALLOC_MAX_FACE; larger boxes get
+ * FDTD_ERR_INVALID.  The first call on each device resolves that array's
+ * device address, so make it before any stream capture.  Calls that overlap
+ * on the GPU share the array and race.  No counterpart in the reference. */
+#define FDTD_NOALLOC_MAX_FACE (1024 * 256)
+int fdtd_dft_rel_change_noalloc(const double *cur, const double *prev, int32_t n_face,
+                                int32_t nfreq, int32_t fi, double *out2, void *stream);
+
 /* Far-field E, H at n_obs points (float64 xyz) from face DFT slice fi:
  * eh[n_obs][6] complex128 = (Ex,Ey,Ez,Hx,Hy,Hz); nl_scratch: n_obs*6 complex128.
  * Direct surface sum in float64 with the kernel's sign (eta N_t - r x L).

@@ -25,6 +25,7 @@ FDTD_F64 = 1
 FDTD_MAX_SOURCES = 8
 FDTD_MAX_PLANES = 4
 FDTD_MAX_FREQS = 64
+FDTD_NOALLOC_MAX_FACE = 1024 * 256
 FDTD_SRC_JX = 0
 FDTD_SRC_EX = 1
 
@@ -77,6 +78,8 @@ SIGNATURES = {
     "fdtd_rel_change_blocks": (c_int32, [c_int32]),
     "fdtd_dft_rel_change": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
                                       c_void_p, c_void_p]),
+    "fdtd_dft_rel_change_noalloc": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_int32,
+                                              c_void_p, c_void_p]),
     "fdtd_farfield": (c_int32, [POINTER(Box), c_void_p, c_int32, c_double, c_double, c_double,
                                 c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "fdtd_last_error": (c_char_p, []),

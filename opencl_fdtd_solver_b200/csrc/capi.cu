@@ -22,6 +22,9 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
                             double k_wave, double eta0, const double *obs, int n_obs,
                             double *nl, double *eh, cudaStream_t st);
 int read_fused_error(int reset);
+int noalloc_rel_max_face();
+cudaError_t launch_rel_change_noalloc(const double *cur, const double *prev, int n, int nfreq,
+                                      int fi, double *out2, cudaStream_t st);
 }  // namespace fdtd
 
 namespace {
@@ -298,6 +301,21 @@ int fdtd_dft_rel_change(const double *cur, const double *prev, int32_t n_face, i
     return cuda_status(fdtd::launch_rel_change(cur, prev, n_face, nfreq, fi, scratch, out2,
                                                (cudaStream_t)stream),
                        "dft_rel_change");
+}
+
+int fdtd_dft_rel_change_noalloc(const double *cur, const double *prev, int32_t n_face,
+                                int32_t nfreq, int32_t fi, double *out2, void *stream) {
+    if (!cur || !prev || !out2) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    if (n_face <= 0 || nfreq <= 0 || fi < 0 || fi >= nfreq)
+        return fail(FDTD_ERR_INVALID, "n_face %d, nfreq %d, fi %d", n_face, nfreq, fi);
+    if (n_face > fdtd::noalloc_rel_max_face())
+        return fail(FDTD_ERR_INVALID,
+                    "n_face %d exceeds the %d face samples the built-in scratch array holds; "
+                    "use fdtd_dft_rel_change with a caller buffer",
+                    n_face, fdtd::noalloc_rel_max_face());
+    return cuda_status(
+        fdtd::launch_rel_change_noalloc(cur, prev, n_face, nfreq, fi, out2, (cudaStream_t)stream),
+        "dft_rel_change_noalloc");
 }
 
 int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl, double k_wave,

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "../../include/fdtd_b200.h"
 
@@ -311,6 +312,57 @@ int rel_change_blocks(int n) {
 cudaError_t launch_rel_change(const double *cur, const double *prev, int n, int nfreq, int fi,
                               double *scratch, double *out2, cudaStream_t st) {
     const int nb = rel_change_blocks(n);
+    k_rel_partial<<<nb, REL_THREADS, 0, st>>>(reinterpret_cast<const double2 *>(cur),
+                                              reinterpret_cast<const double2 *>(prev), n, nfreq,
+                                              fi, scratch);
+    k_rel_final<<<1, REL_THREADS, 0, st>>>(scratch, nb, out2);
+    return cudaGetLastError();
+}
+
+// ---- relative change without caller-provided scratch ---------------------
+//
+// Same two-pass reduction as launch_rel_change, but the per-block partial sums
+// live in this file-scope device array instead of a buffer the caller
+// allocates.  It holds NOALLOC_REL_BLOCKS blocks (16 KiB of doubles) on every
+// GPU that loads the library, for the life of the process.  One partial per
+// block of 256 face samples, so n_face is limited to NOALLOC_REL_BLOCKS * 256.
+// Each call writes every partial it reads back, so nothing needs clearing
+// between calls; calls that overlap on the GPU share the array and race.
+constexpr int NOALLOC_REL_BLOCKS = 1024;
+static __device__ __align__(256) double g_rel_scratch[2 * NOALLOC_REL_BLOCKS];
+
+int noalloc_rel_max_face() { return NOALLOC_REL_BLOCKS * REL_THREADS; }
+
+namespace {
+std::mutex g_scratch_mu;
+double *g_scratch_ptr[256];  // device address of g_rel_scratch, per device ordinal
+}  // namespace
+
+// Device address of the scratch array on the current device.  The first call
+// on a device resolves it with cudaGetSymbolAddress (host code must not use the
+// array's name as a device pointer: it is only a host-side stand-in).
+cudaError_t noalloc_rel_scratch(double **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_rel_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launch_rel_change_noalloc(const double *cur, const double *prev, int n, int nfreq,
+                                      int fi, double *out2, cudaStream_t st) {
+    double *scratch = nullptr;
+    cudaError_t e = noalloc_rel_scratch(&scratch);
+    if (e != cudaSuccess) return e;
+    const int nb = (n + REL_THREADS - 1) / REL_THREADS;
     k_rel_partial<<<nb, REL_THREADS, 0, st>>>(reinterpret_cast<const double2 *>(cur),
                                               reinterpret_cast<const double2 *>(prev), n, nfreq,
                                               fi, scratch);
