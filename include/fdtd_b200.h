@@ -184,6 +184,71 @@ int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl,
                   double k_wave, double eta0, const double *obs_xyz, int32_t n_obs,
                   double *nl_scratch, double *eh, void *stream);
 
+/* ---- adjoint (ε-gradient) ------------------------------------------------ */
+/* No reference counterpart: the reference has no gradient.  These entry points
+ * run the reverse-time sweep of the transposed (discrete adjoint) Yee/CPML
+ * step of fdtd_step / fdtd_update_H + fdtd_update_E for a lossless grid
+ * (grid.lossy must be 0).  With Ē, H̄ the adjoints of E^{n+1}, H^{n+1/2} and
+ * P the adjoints of the ψ recursions, one reverse step is
+ *   H̄ += B^T ḡ(Ē, P_E),   P_E' = b_e P_E ± ce Ē          (transposed E update)
+ *   Ē += F^T ā(H̄, P_H),   P_H' = b_h P_H ∓ dtm H̄         (transposed H update)
+ * where B, F are the backward / forward differences of yee_update.cl:145-150
+ * and :30-35 (zero at index 0 / at the last index). */
+
+/* Adjoint state.  E/H are updated in place; the P stripes have the ψ stripe
+ * shapes and order of fdtd_cpml and are ping-ponged: a step reads pe/ph and
+ * writes pe_next/ph_next (which must not alias them). */
+typedef struct {
+    void *E[3];
+    void *H[3];
+    const void *pe[6];
+    void *pe_next[6];
+    const void *ph[6];
+    void *ph_next[6];
+    const void *ce[3];      /* the forward's dt/(eps0 eps_edge)                */
+} fdtd_adjoint_fields;
+
+/* Adjoint source of a real objective J(D) of plane-DFT samples
+ * D[c][f][a][b] = Σ_m phase_m[f] E_c^m over the patch [a0,a1) x [b0,b1) of
+ * the plane axis = index (a, b: the two other axes in x, y, z order).
+ * seed[c][f][a][b] (complex128) = ∂J/∂Re D + i ∂J/∂Im D, components in
+ * Ex, Ey, Ez bit order of comp_mask (E only).  phase: nfreq complex128 values,
+ * the phase the forward DFT applied to the E^m this call seeds.  Adds
+ * ∂J/∂E^m = Re(seed)·Re(phase) + Im(seed)·Im(phase) to Ē. */
+typedef struct {
+    int32_t axis, index, a0, a1, b0, b1, comp_mask, nfreq;
+    const double *seed;
+    const double *phase;
+} fdtd_adjoint_seed;
+
+/* Gradient box [lo, hi) of E edges (all three components).  e_next / e_prev
+ * are the forward's E^{n+1} and E^n over the box, laid out [3][box cells] in
+ * C order (fdtd_capture_box); g[3][box cells] float64 accumulates
+ * Σ_n Ē^{n+1}·(E^{n+1} − E^n), which equals ce·∂J/∂ce for a lossless grid,
+ * sheet injections included. */
+typedef struct {
+    int32_t lo[3], hi[3];
+    const void *e_next;
+    const void *e_prev;
+    double *g;
+} fdtd_grad_box;
+
+/* Copy E over box [lo, hi) into out ([3][box cells], field dtype). */
+int fdtd_capture_box(const fdtd_grid *g, const void *const E[3], const int32_t lo[3],
+                     const int32_t hi[3], void *out, void *stream);
+
+/* Ē += ∂J/∂E^m for one seed (used once before the first reverse step). */
+int fdtd_adjoint_seed_add(const fdtd_grid *g, void *const Ebar[3],
+                          const fdtd_adjoint_seed *seed, void *stream);
+
+/* One reverse step n: on entry Ē = ∂J/∂E^{n+1} (complete), H̄ = ∂J/∂H^{n+1/2}
+ * from later steps.  Runs the transposed E update (accumulating gb when
+ * non-NULL), then the transposed H update, then adds next_seed (the objective's
+ * ∂J/∂E^n, may be NULL).  On return Ē = ∂J/∂E^n and H̄ = ∂J/∂H^{n−1/2}. */
+int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fdtd_cpml *c,
+                      const fdtd_grad_box *gb, const fdtd_adjoint_seed *next_seed,
+                      void *stream);
+
 /* ---- diagnostics --------------------------------------------------------- */
 
 /* Message for the last non-OK status returned on this host thread. */

@@ -8,14 +8,16 @@ with ``CUDAFDTD`` / ``CUDANear2FarMonitor`` in place of the OpenCL classes):
 * ``CUDANear2FarMonitor`` — Huygens-box DFT + far field
 * ``CUDAPlaneDFTMonitor`` — single-plane DFT fused into the E update
 * ``StepCallback``, ``SourceMonitorMixin``, ``BACKENDS``, ``get_backend``
-* ``near2far_contract`` — tensor-core near-to-far contraction
-* ``EpsilonObjective`` — adjoint ε-gradient behind ``torch.autograd.Function``
+* ``DFTObjective``, ``EpsilonAdjoint``, ``EpsilonObjective`` — discrete-adjoint
+  ε-gradient of a plane-DFT objective (``EpsilonObjective`` is the
+  ``torch.autograd.Function``)
 
 Importing the package does not touch CUDA; constructing an engine does.
 """
 
 __version__ = "0.1.0"
 
+from .adjoint import DFTObjective, EpsilonAdjoint, EpsilonObjective, epsilon_objective
 from .constants import C0, EPS0, ETA0, MU0
 from .engine import CUDAFDTD
 from .monitors import CUDANear2FarMonitor, CUDAPlaneDFTMonitor
@@ -34,5 +36,9 @@ __all__ = [
     "BACKENDS",
     "get_backend",
     "register_backend",
+    "DFTObjective",
+    "EpsilonAdjoint",
+    "EpsilonObjective",
+    "epsilon_objective",
     "__version__",
 ]

@@ -65,6 +65,22 @@ class Box(Structure):
                 ("nfreq", c_int32)]
 
 
+class AdjointFields(Structure):
+    _fields_ = [("E", V3), ("H", V3), ("pe", V6), ("pe_next", V6), ("ph", V6), ("ph_next", V6),
+                ("ce", V3)]
+
+
+class AdjointSeed(Structure):
+    _fields_ = [("axis", c_int32), ("index", c_int32), ("a0", c_int32), ("a1", c_int32),
+                ("b0", c_int32), ("b1", c_int32), ("comp_mask", c_int32), ("nfreq", c_int32),
+                ("seed", c_void_p), ("phase", c_void_p)]
+
+
+class GradBox(Structure):
+    _fields_ = [("lo", c_int32 * 3), ("hi", c_int32 * 3), ("e_next", c_void_p),
+                ("e_prev", c_void_p), ("g", c_void_p)]
+
+
 # name -> (restype, argtypes); every symbol include/fdtd_b200.h declares.
 SIGNATURES = {
     "fdtd_update_H": (c_int32, [POINTER(Grid), POINTER(Fields), POINTER(Cpml), c_void_p]),
@@ -82,6 +98,12 @@ SIGNATURES = {
                                               c_void_p, c_void_p]),
     "fdtd_farfield": (c_int32, [POINTER(Box), c_void_p, c_int32, c_double, c_double, c_double,
                                 c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    "fdtd_capture_box": (c_int32, [POINTER(Grid), POINTER(c_void_p), POINTER(c_int32),
+                                   POINTER(c_int32), c_void_p, c_void_p]),
+    "fdtd_adjoint_seed_add": (c_int32, [POINTER(Grid), POINTER(c_void_p), POINTER(AdjointSeed),
+                                        c_void_p]),
+    "fdtd_adjoint_step": (c_int32, [POINTER(Grid), POINTER(AdjointFields), POINTER(Cpml),
+                                    POINTER(GradBox), POINTER(AdjointSeed), c_void_p]),
     "fdtd_last_error": (c_char_p, []),
     "fdtd_device_status": (c_int32, [POINTER(c_int32), c_int32]),
     "fdtd_version": (c_char_p, []),

@@ -1,0 +1,345 @@
+"""ε-gradients of plane-DFT objectives by the discrete adjoint of the Yee/CPML step.
+
+The reference solver (r-bridge/opencl-fdtd-solver) has no gradient.  This module adds
+one on top of :class:`CUDAFDTD` without changing the forward path:
+
+* ``EpsilonAdjoint.forward(eps_design)`` sets ``εr`` (background outside the design
+  box), runs ``n_steps`` from rest with the engine's registered sources, accumulates
+  a plane DFT on the objective plane (the same kernel and phase recurrence as
+  :class:`CUDAPlaneDFTMonitor`, reference ``monitors.py:571-584``), evaluates
+  ``J = fn(D)`` on the patch and keeps a checkpoint of the full state every
+  ``checkpoint_every`` steps (fields and ψ stripes: ``CUDAFDTD.save_state``).
+* ``backward()`` runs the adjoint sweep: ``∂J/∂D`` (by torch autograd through ``fn``)
+  seeds ``Ē`` on the patch each step (``fdtd_adjoint_seed_add`` / the seed of
+  ``fdtd_adjoint_step``); segments are replayed from their checkpoints, newest
+  first, with ``E`` captured over the design's edge box each step
+  (``fdtd_capture_box``), and the transposed step runs backwards through the segment
+  (``fdtd_adjoint_step``), accumulating ``Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce``
+  on the edge box in float64.  The host chain rule through ``ce = dt/(ε0·ε_edge)``
+  and the two-cell edge average (reference ``materials.py:28-56``) gives
+  ``∂J/∂εr`` per design cell.
+* :class:`EpsilonObjective` wraps the pair as a ``torch.autograd.Function``.
+
+The gradient is exact for the discrete scheme (lossless grids: ``set_epsilon``
+without σ); its cost is one forward solve, one replayed forward solve and one
+adjoint sweep.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi as capi
+from .engine import CUDAFDTD
+from .monitors import CUDAPlaneDFTMonitor
+
+E_NAMES = ("Ex", "Ey", "Ez")
+
+
+def _default_fn(D):
+    return (D.real ** 2 + D.imag ** 2).sum()
+
+
+class DFTObjective:
+    """``J = fn(D)`` of the plane DFT ``D`` over a patch.
+
+    axis, index : the plane (``axis`` 0/1/2 or 'x'/'y'/'z')
+    patch       : ``((a0, a1), (b0, b1))`` half-open ranges over the two other axes
+                  in x, y, z order
+    freqs       : DFT frequencies (Hz)
+    components  : E components (``'Ex'``, ``'Ey'``, ``'Ez'``)
+    fn          : differentiable torch function of the complex128 tensor
+                  ``D[component][freq][a][b]`` returning a real scalar; default
+                  ``Σ|D|²``
+    """
+
+    def __init__(self, axis, index, patch, freqs, components=("Ex",), fn=None):
+        self.axis = {"x": 0, "y": 1, "z": 2}.get(axis, axis)
+        if self.axis not in (0, 1, 2):
+            raise ValueError(f"axis must be 0, 1, 2 or 'x', 'y', 'z'; got {axis!r}")
+        self.index = int(index)
+        (a0, a1), (b0, b1) = patch
+        self.patch = ((int(a0), int(a1)), (int(b0), int(b1)))
+        self.freqs = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+        if not 0 < self.freqs.size <= capi.FDTD_MAX_FREQS:
+            raise ValueError(f"1 to {capi.FDTD_MAX_FREQS} frequencies, got {self.freqs.size}")
+        comps = (components,) if isinstance(components, str) else tuple(components)
+        for c in comps:
+            if c not in E_NAMES:
+                raise ValueError(f"objective components must be E components, got {c!r}")
+        self.components = tuple(c for c in E_NAMES if c in comps)
+        self.comp_mask = sum(1 << E_NAMES.index(c) for c in self.components)
+        self.fn = _default_fn if fn is None else fn
+
+
+def _phase_sequence(freqs, dt, n_steps, t_first):
+    """E phases of the plane DFT per step (complex128 ``(n_steps, nfreq)``), with the
+    recurrence of ``CUDAPlaneDFTMonitor``: ``e^{jωt_first}·dt``, then ``·e^{jωdt}``."""
+    omega = 2.0 * np.pi * np.asarray(freqs, np.float64)
+    d = np.exp(1j * omega * float(dt))
+    out = np.empty((int(n_steps), omega.size), np.complex128)
+    p = np.exp(1j * omega * float(t_first)) * float(dt)
+    for n in range(int(n_steps)):
+        if n > 0:
+            p = p * d
+        out[n] = p
+    return out
+
+
+def _edge_eps(eps):
+    ex = eps.copy()
+    ex[:-1] = 0.5 * (eps[:-1] + eps[1:])
+    ey = eps.copy()
+    ey[:, :-1] = 0.5 * (eps[:, :-1] + eps[:, 1:])
+    ez = eps.copy()
+    ez[:, :, :-1] = 0.5 * (eps[:, :, :-1] + eps[:, :, 1:])
+    return ex, ey, ez
+
+
+def edge_to_cells(G, eps_full, design, box):
+    """``ce·∂J/∂ce`` on the edge box (``G[3][box]``) → ``∂J/∂εr`` per design cell.
+
+    ``ce = dt/(ε0·ε_edge)`` gives ``∂J/∂ε_edge = −G/ε_edge``; ``ε_edge`` is the mean of
+    the two cells sharing the edge, the last plane keeping the cell value
+    (reference ``materials.py:28-41``), so each cell collects half of its two edges
+    along each axis (all of the last-plane edge).
+    """
+    eps_e = _edge_eps(eps_full)
+    shape = eps_full.shape
+    bsl = tuple(slice(lo, hi) for lo, hi in box)
+    dsl = tuple(slice(lo, hi) for lo, hi in design)
+    out = np.zeros(tuple(hi - lo for lo, hi in design), np.float64)
+    for c in range(3):
+        ge = np.zeros(shape, np.float64)
+        ge[bsl] = -G[c] / eps_e[c][bsl]
+        n = shape[c]
+        cell = np.zeros(shape, np.float64)
+        dst = [slice(None)] * 3
+        src = [slice(None)] * 3
+        dst[c] = slice(0, n - 1)
+        cell[tuple(dst)] += 0.5 * ge[tuple(dst)]      # edge i   -> cell i
+        dst[c] = slice(1, n)
+        src[c] = slice(0, n - 1)
+        cell[tuple(dst)] += 0.5 * ge[tuple(src)]      # edge i-1 -> cell i
+        dst[c] = slice(n - 1, n)
+        cell[tuple(dst)] += ge[tuple(dst)]            # last plane
+        out += cell[dsl]
+    return out
+
+
+class EpsilonAdjoint:
+    """Objective and discrete-adjoint gradient with respect to ``εr`` in a design box.
+
+    fdtd             : a :class:`CUDAFDTD` with its sources registered (source
+                       callbacks must depend only on ``fdtd.t``: segments are replayed)
+    design           : ``((i0, i1), (j0, j1), (k0, k1))`` half-open design box
+    n_steps          : time steps per solve (from rest at t = 0)
+    objective        : :class:`DFTObjective`
+    eps_background   : cell-centred ``εr`` outside the design box (default 1)
+    checkpoint_every : steps per replayed segment (K)
+
+    The engine's own monitors are detached while this object steps it.
+    """
+
+    def __init__(self, fdtd, design, n_steps, objective, *, eps_background=None,
+                 checkpoint_every=100):
+        if not isinstance(fdtd, CUDAFDTD):
+            raise TypeError("EpsilonAdjoint needs a CUDAFDTD engine")
+        self.fdtd = fdtd
+        shape = (fdtd.Nx, fdtd.Ny, fdtd.Nz)
+        self.design = tuple((int(lo), int(hi)) for lo, hi in design)
+        if len(self.design) != 3 or any(not (0 <= lo < hi <= n)
+                                        for (lo, hi), n in zip(self.design, shape)):
+            raise ValueError(f"design box {design} is empty or outside the grid {shape}")
+        self.n_steps = int(n_steps)
+        if self.n_steps < 1:
+            raise ValueError("n_steps must be >= 1")
+        self.K = int(checkpoint_every)
+        if self.K < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        if not isinstance(objective, DFTObjective):
+            raise TypeError("objective must be a DFTObjective")
+        self.objective = objective
+        o = objective
+        dims = list(shape)
+        if not 0 <= o.index < dims[o.axis]:
+            raise ValueError(f"objective plane index {o.index} outside [0, {dims[o.axis]})")
+        del dims[o.axis]
+        (a0, a1), (b0, b1) = o.patch
+        if not (0 <= a0 < a1 <= dims[0] and 0 <= b0 < b1 <= dims[1]):
+            raise ValueError(f"objective patch {o.patch} is empty or outside the plane {dims}")
+        if eps_background is None:
+            self.eps_background = np.ones(shape, np.float64)
+        else:
+            self.eps_background = np.array(eps_background, dtype=np.float64)
+            if self.eps_background.shape != shape:
+                raise ValueError(f"eps_background shape {self.eps_background.shape} != {shape}")
+        # edge box: every edge a design cell's ε reaches
+        self.box = tuple((max(0, lo - 1), hi) for lo, hi in self.design)
+        self.box_shape = tuple(hi - lo for lo, hi in self.box)
+        self._ckpts = None
+        self._seed = None
+        self.J = None
+        self.D = None
+
+    # ----------------------------------------------------------------- forward
+    def _eps_full(self, eps_design):
+        eps = np.asarray(eps_design, dtype=np.float64)
+        want = tuple(hi - lo for lo, hi in self.design)
+        if eps.shape != want:
+            raise ValueError(f"eps_design shape {eps.shape} != design box shape {want}")
+        full = self.eps_background.copy()
+        full[tuple(slice(lo, hi) for lo, hi in self.design)] = eps
+        return full
+
+    def forward(self, eps_design):
+        """Solve with ``εr = eps_design`` in the design box; return ``J`` (float)."""
+        fd = self.fdtd
+        o = self.objective
+        self._eps = self._eps_full(eps_design)
+        fd.set_epsilon(self._eps)
+        fd.reset_state()
+        saved = fd._monitors
+        fd._monitors = []
+        ckpts = []
+        try:
+            mon = CUDAPlaneDFTMonitor(fd, o.axis, o.index, o.freqs, o.components)
+            self._t_first = fd.t + fd.dt
+            for n in range(self.n_steps):
+                if n % self.K == 0:
+                    ckpts.append(fd.save_state())
+                fd.step()
+        finally:
+            fd._monitors = saved
+        self._ckpts = ckpts
+        (a0, a1), (b0, b1) = o.patch
+        D = torch.view_as_complex(mon.acc)[:, :, a0:a1, b0:b1].detach().clone()
+        Dg = D.clone().requires_grad_(True)
+        with torch.enable_grad():
+            J = o.fn(Dg)
+            (seed,) = torch.autograd.grad(J, Dg)
+        self._seed = torch.view_as_real(seed.detach().to(torch.complex128)).contiguous()
+        self.D = D
+        self.J = float(J.detach())
+        return self.J
+
+    # ---------------------------------------------------------------- backward
+    def _adjoint_buffers(self):
+        fd = self.fdtd
+        tdt = fd._tdt
+        shp = (fd.Nx, fd.Ny, fd.Nz)
+        z = lambda s: torch.zeros(s, dtype=tdt, device=fd.device)  # noqa: E731
+        Eb = [z(shp) for _ in range(3)]
+        Hb = [z(shp) for _ in range(3)]
+        stripes = [tuple(p.shape) for p in fd._psi_e]
+        PE = [[z(s) for s in stripes] for _ in range(2)]
+        PH = [[z(s) for s in stripes] for _ in range(2)]
+        fields = []
+        for par in range(2):
+            f = capi.AdjointFields()
+            for c in range(3):
+                f.E[c] = Eb[c].data_ptr()
+                f.H[c] = Hb[c].data_ptr()
+                f.ce[c] = fd._ce[c].data_ptr()
+            for q in range(6):
+                f.pe[q] = PE[par][q].data_ptr()
+                f.pe_next[q] = PE[par ^ 1][q].data_ptr()
+                f.ph[q] = PH[par][q].data_ptr()
+                f.ph_next[q] = PH[par ^ 1][q].data_ptr()
+            fields.append(f)
+        return Eb, Hb, PE, PH, fields
+
+    def backward(self, grad_output=1.0):
+        """``grad_output · ∂J/∂εr`` over the design box (float64 NumPy array)."""
+        if self._ckpts is None:
+            raise RuntimeError("call forward() before backward()")
+        fd = self.fdtd
+        o = self.objective
+        if fd.lossy:
+            raise NotImplementedError("the adjoint gradient needs a lossless grid")
+        st = fd.queue.cuda_stream
+        N, K = self.n_steps, self.K
+        with torch.cuda.stream(fd.queue):
+            Eb, Hb, PE, PH, fields = self._adjoint_buffers()
+            phases = _phase_sequence(o.freqs, fd.dt, N, self._t_first)
+            ph_dev = torch.from_numpy(np.ascontiguousarray(
+                np.stack([phases.real, phases.imag], -1))).to(fd.device)
+            G = torch.zeros((3, *self.box_shape), dtype=torch.float64, device=fd.device)
+            cap = torch.empty((K + 1, 3, *self.box_shape), dtype=fd._tdt, device=fd.device)
+        (a0, a1), (b0, b1) = o.patch
+        sd = capi.AdjointSeed(axis=o.axis, index=o.index, a0=a0, a1=a1, b0=b0, b1=b1,
+                              comp_mask=o.comp_mask, nfreq=o.freqs.size,
+                              seed=self._seed.data_ptr(), phase=0)
+        ph_stride = o.freqs.size * 2 * 8
+        ph0 = ph_dev.data_ptr()
+        gb = capi.GradBox()
+        for a in range(3):
+            gb.lo[a], gb.hi[a] = self.box[a]
+        gb.g = G.data_ptr()
+        lo = (ctypes.c_int32 * 3)(*[b[0] for b in self.box])
+        hi = (ctypes.c_int32 * 3)(*[b[1] for b in self.box])
+        cap_stride = cap[0].numel() * cap.element_size()
+        cap0 = cap.data_ptr()
+        grid, cpml = fd._grid, fd._cpml_base
+        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb])
+        sd.phase = ph0 + (N - 1) * ph_stride
+        capi.run("fdtd_adjoint_seed_add", grid, Ebp, sd, st)
+        saved = fd._monitors
+        fd._monitors = []
+        par = 0
+        try:
+            for s in range(len(self._ckpts) - 1, -1, -1):
+                n0 = s * K
+                n1 = min(N, n0 + K)
+                fd.load_state(self._ckpts[s])
+                for m in range(n1 - n0 + 1):
+                    if m > 0:
+                        fd.step()
+                    Ep = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in fd._E])
+                    capi.run("fdtd_capture_box", grid, Ep, lo, hi, cap0 + m * cap_stride, st)
+                for n in range(n1 - 1, n0 - 1, -1):
+                    gb.e_next = cap0 + (n + 1 - n0) * cap_stride
+                    gb.e_prev = cap0 + (n - n0) * cap_stride
+                    if n >= 1:
+                        sd.phase = ph0 + (n - 1) * ph_stride
+                        seed_arg = ctypes.byref(sd)
+                    else:
+                        seed_arg = None
+                    capi.run("fdtd_adjoint_step", grid, fields[par], cpml, gb, seed_arg, st)
+                    par ^= 1
+        finally:
+            fd._monitors = saved
+        fd.queue.synchronize()
+        self._adjoint_state = (Eb, Hb)
+        g_edges = G.cpu().numpy()
+        return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)
+
+    def value_and_grad(self, eps_design):
+        """``(J, ∂J/∂εr)`` in one forward + adjoint pass."""
+        J = self.forward(eps_design)
+        return J, self.backward()
+
+
+class EpsilonObjective(torch.autograd.Function):
+    """``J = EpsilonObjective.apply(eps_design, adjoint)``: autograd through the solver."""
+
+    @staticmethod
+    def forward(ctx, eps_design, adjoint):
+        J = adjoint.forward(eps_design.detach().cpu().numpy())
+        ctx.adjoint = adjoint
+        ctx.meta = (eps_design.dtype, eps_design.device)
+        return torch.tensor(J, dtype=torch.float64, device=eps_design.device)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        g = ctx.adjoint.backward(float(grad_out))
+        dtype, device = ctx.meta
+        return torch.as_tensor(g, device=device).to(dtype), None
+
+
+def epsilon_objective(eps_design, adjoint):
+    """Functional form of :class:`EpsilonObjective`."""
+    return EpsilonObjective.apply(eps_design, adjoint)

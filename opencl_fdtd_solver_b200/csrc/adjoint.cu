@@ -1,0 +1,309 @@
+// Discrete adjoint of the Yee/CPML step (reverse-time sweep for ε-gradients).
+//
+// The forward step (yee_update.cl:11-238 as restated in yee_cell.cuh) is, for a
+// lossless grid and fixed coefficients, a linear map of (E, H, ψ_E, ψ_H).  Its
+// transpose is applied here in the reverse order of the forward operations:
+//
+//   transposed E update (k_adj_H):  for every E pair p (component c, derivative
+//     axis d; ψ_E order Ex_y, Ex_z, Ey_x, Ey_z, Ez_x, Ez_y)
+//       P_p' = b_e,d·P_p + s_p·ce_c·Ē_c                 (adjoint ψ recursion)
+//       ḡ_p  = s_p·ce_c·ik_e,d·Ē_c + c_e,d·P_p'          (P term in the d slab only)
+//       H̄   += B_d^T ḡ_p                                 (backward difference, transposed)
+//   transposed H update (k_adj_E):  for every H pair p (ψ_H order Hx_y … Hz_y)
+//       P_p' = b_h,d·P_p + s'_p·dtm·H̄_c
+//       ā_p  = s'_p·dtm·ik_h,d·H̄_c + c_h,d·P_p'
+//       Ē   += F_d^T ā_p                                 (forward difference, transposed)
+//
+// with s = (+,−,−,+,+,−) for the E pairs and s' = −s for the H pairs (the signs
+// of each term in the forward update).  B_d zeroes index 0 and F_d the last
+// index (yee_update.cl:30-35, 145-150), so
+//   (B_d^T v)(x) = [x ≥ 1]·v(x) − [x ≤ n−2]·v(x+1),
+//   (F_d^T v)(x) = [x ≥ 1]·v(x−1) − [x ≤ n−2]·v(x).
+// P is carried in the ψ stripe layout and ping-ponged, so that a thread may read
+// its neighbours' P while writing its own.
+//
+// ε enters through ce = dt/(ε0·ε_edge).  For ca ≡ 1, ∂E^{n+1}/∂ce = (E^{n+1} − E^n)/ce
+// (the sheet term −ce·J·w of sources.cl:48 included), so the gradient box
+// accumulates Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce in float64.
+//
+// Compiled with --fmad=false (build.py) so that every product and sum rounds
+// separately, in the order written, like the CPU restatement the tests hold it to.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/fdtd_b200.h"
+#include "adjoint.cuh"
+
+namespace fdtd {
+
+constexpr int ADJ_TK = 32;
+constexpr int ADJ_TJ = 8;
+
+// Derivative axis of pair p (the same for the E and H orders).
+__host__ __device__ constexpr int pair_axis(int p) {
+    return (p == 2 || p == 4) ? 0 : ((p == 0 || p == 5) ? 1 : 2);
+}
+// Sign of pair p in the forward E update (+ for Ex_y, Ey_z, Ez_x).
+__host__ __device__ constexpr bool pair_pos_e(int p) { return p == 0 || p == 3 || p == 4; }
+
+template <int D>
+__device__ __forceinline__ int64_t stripe_index(int i, int j, int k, int nx, int ny, int nz,
+                                                int npml) {
+    if (D == 0) return psi_x_index(i, j, k, nx, ny, nz, npml);
+    if (D == 1) return psi_y_index(i, j, k, ny, nz, npml);
+    return psi_z_index(i, j, k, ny, nz, npml);
+}
+
+// ḡ of E pair P at cell (i, j, k) with adjoint field eb and coefficient ce.
+// OWN: this thread owns the cell and writes its advanced P.
+template <typename T, int P, bool OWN>
+__device__ __forceinline__ T e_pair(const AdjArgs<T> &a, int i, int j, int k, T eb, T ce) {
+    constexpr int D = pair_axis(P);
+    constexpr bool POS = pair_pos_e(P);
+    const int x = D == 0 ? i : (D == 1 ? j : k);
+    const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
+    const T t = ce * a.cpe.ik[D][x] * eb;
+    T g = POS ? t : -t;
+    if (in_slab(x, n, a.npml)) {
+        const int64_t s = stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml);
+        const T u = ce * eb;
+        const T pn = a.cpe.b[D][x] * a.pe[P][s] + (POS ? u : -u);
+        if (OWN) a.pe_next[P][s] = pn;
+        g = g + a.cpe.c[D][x] * pn;
+    }
+    return g;
+}
+
+// ā of H pair P at cell (i, j, k) with adjoint field hb.
+template <typename T, int P, bool OWN>
+__device__ __forceinline__ T h_pair(const AdjArgs<T> &a, int i, int j, int k, T hb) {
+    constexpr int D = pair_axis(P);
+    constexpr bool POS = !pair_pos_e(P);
+    const int x = D == 0 ? i : (D == 1 ? j : k);
+    const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
+    const T t = a.dtm * a.cph.ik[D][x] * hb;
+    T g = POS ? t : -t;
+    if (in_slab(x, n, a.npml)) {
+        const int64_t s = stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml);
+        const T u = a.dtm * hb;
+        const T pn = a.cph.b[D][x] * a.ph[P][s] + (POS ? u : -u);
+        if (OWN) a.ph_next[P][s] = pn;
+        g = g + a.cph.c[D][x] * pn;
+    }
+    return g;
+}
+
+// Objective seed for E cell (i, j, k): Ē_c += Σ_f Re(seed)·Re(phase) + Im(seed)·Im(phase).
+template <typename T>
+__device__ __forceinline__ void add_seed(const AdjSeed &sd, int i, int j, int k, T &ex, T &ey,
+                                         T &ez) {
+    const int w = sd.axis == 0 ? i : (sd.axis == 1 ? j : k);
+    if (w != sd.index) return;
+    const int pa = sd.axis == 0 ? j : i;
+    const int pb = sd.axis == 2 ? j : k;
+    if (pa < sd.a0 || pa >= sd.a1 || pb < sd.b0 || pb >= sd.b1) return;
+    const int64_t np = (int64_t)(sd.a1 - sd.a0) * (sd.b1 - sd.b0);
+    const int64_t loc = (int64_t)(pa - sd.a0) * (sd.b1 - sd.b0) + (pb - sd.b0);
+    int slot = 0;
+    for (int c = 0; c < 3; ++c) {
+        if (!(sd.comp_mask & (1 << c))) continue;
+        double acc = 0.0;
+        for (int f = 0; f < sd.nfreq; ++f) {
+            const double *s = sd.seed + 2 * (((int64_t)slot * sd.nfreq + f) * np + loc);
+            acc = acc + (s[0] * sd.phase[2 * f] + s[1] * sd.phase[2 * f + 1]);
+        }
+        if (c == 0) ex = ex + (T)acc;
+        if (c == 1) ey = ey + (T)acc;
+        if (c == 2) ez = ez + (T)acc;
+        ++slot;
+    }
+}
+
+// Transposed E update: H̄ += B^T ḡ(Ē, P_E); P_E advanced; gradient accumulated.
+template <typename T>
+__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<T> gb) {
+    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
+    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
+    const int i = blockIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (k >= nz || j >= ny) return;
+    const int64_t sx = (int64_t)ny * nz, sy = nz;
+    const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
+    const T ex = a.E[0][idx], ey = a.E[1][idx], ez = a.E[2][idx];
+    const T cx = a.ce[0][idx], cy = a.ce[1][idx], cz = a.ce[2][idx];
+    const T g0 = e_pair<T, 0, true>(a, i, j, k, ex, cx);
+    const T g1 = e_pair<T, 1, true>(a, i, j, k, ex, cx);
+    const T g2 = e_pair<T, 2, true>(a, i, j, k, ey, cy);
+    const T g3 = e_pair<T, 3, true>(a, i, j, k, ey, cy);
+    const T g4 = e_pair<T, 4, true>(a, i, j, k, ez, cz);
+    const T g5 = e_pair<T, 5, true>(a, i, j, k, ez, cz);
+    T g1n = T(0), g3n = T(0), g0n = T(0), g5n = T(0), g2n = T(0), g4n = T(0);
+    if (k <= nz - 2) {
+        g1n = e_pair<T, 1, false>(a, i, j, k + 1, a.E[0][idx + 1], a.ce[0][idx + 1]);
+        g3n = e_pair<T, 3, false>(a, i, j, k + 1, a.E[1][idx + 1], a.ce[1][idx + 1]);
+    }
+    if (j <= ny - 2) {
+        g0n = e_pair<T, 0, false>(a, i, j + 1, k, a.E[0][idx + sy], a.ce[0][idx + sy]);
+        g5n = e_pair<T, 5, false>(a, i, j + 1, k, a.E[2][idx + sy], a.ce[2][idx + sy]);
+    }
+    if (i <= nx - 2) {
+        g2n = e_pair<T, 2, false>(a, i + 1, j, k, a.E[1][idx + sx], a.ce[1][idx + sx]);
+        g4n = e_pair<T, 4, false>(a, i + 1, j, k, a.E[2][idx + sx], a.ce[2][idx + sx]);
+    }
+    const T tz3 = (k >= 1 ? g3 : T(0)) - g3n;
+    const T ty5 = (j >= 1 ? g5 : T(0)) - g5n;
+    const T tz1 = (k >= 1 ? g1 : T(0)) - g1n;
+    const T tx4 = (i >= 1 ? g4 : T(0)) - g4n;
+    const T ty0 = (j >= 1 ? g0 : T(0)) - g0n;
+    const T tx2 = (i >= 1 ? g2 : T(0)) - g2n;
+    a.H[0][idx] = a.H[0][idx] + (tz3 + ty5);
+    a.H[1][idx] = a.H[1][idx] + (tz1 + tx4);
+    a.H[2][idx] = a.H[2][idx] + (ty0 + tx2);
+    if (gb.active && i >= gb.lo[0] && i < gb.hi[0] && j >= gb.lo[1] && j < gb.hi[1] &&
+        k >= gb.lo[2] && k < gb.hi[2]) {
+        const int by = gb.hi[1] - gb.lo[1], bz = gb.hi[2] - gb.lo[2];
+        const int64_t nb = (int64_t)(gb.hi[0] - gb.lo[0]) * by * bz;
+        const int64_t loc = ((int64_t)(i - gb.lo[0]) * by + (j - gb.lo[1])) * bz + (k - gb.lo[2]);
+        const T ev[3] = {ex, ey, ez};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t q = c * nb + loc;
+            const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
+            gb.g[q] = gb.g[q] + (double)ev[c] * de;
+        }
+    }
+}
+
+// Transposed H update: Ē += F^T ā(H̄, P_H); P_H advanced; then the next seed.
+template <typename T>
+__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed sd) {
+    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
+    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
+    const int i = blockIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    if (k >= nz || j >= ny) return;
+    const int64_t sx = (int64_t)ny * nz, sy = nz;
+    const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
+    const T hx = a.H[0][idx], hy = a.H[1][idx], hz = a.H[2][idx];
+    const T a0 = h_pair<T, 0, true>(a, i, j, k, hx);
+    const T a1 = h_pair<T, 1, true>(a, i, j, k, hx);
+    const T a2 = h_pair<T, 2, true>(a, i, j, k, hy);
+    const T a3 = h_pair<T, 3, true>(a, i, j, k, hy);
+    const T a4 = h_pair<T, 4, true>(a, i, j, k, hz);
+    const T a5 = h_pair<T, 5, true>(a, i, j, k, hz);
+    T a1p = T(0), a3p = T(0), a0p = T(0), a5p = T(0), a2p = T(0), a4p = T(0);
+    if (k >= 1) {
+        a1p = h_pair<T, 1, false>(a, i, j, k - 1, a.H[0][idx - 1]);
+        a3p = h_pair<T, 3, false>(a, i, j, k - 1, a.H[1][idx - 1]);
+    }
+    if (j >= 1) {
+        a0p = h_pair<T, 0, false>(a, i, j - 1, k, a.H[0][idx - sy]);
+        a5p = h_pair<T, 5, false>(a, i, j - 1, k, a.H[2][idx - sy]);
+    }
+    if (i >= 1) {
+        a2p = h_pair<T, 2, false>(a, i - 1, j, k, a.H[1][idx - sx]);
+        a4p = h_pair<T, 4, false>(a, i - 1, j, k, a.H[2][idx - sx]);
+    }
+    const T fz3 = a3p - (k <= nz - 2 ? a3 : T(0));
+    const T fy5 = a5p - (j <= ny - 2 ? a5 : T(0));
+    const T fz1 = a1p - (k <= nz - 2 ? a1 : T(0));
+    const T fx4 = a4p - (i <= nx - 2 ? a4 : T(0));
+    const T fy0 = a0p - (j <= ny - 2 ? a0 : T(0));
+    const T fx2 = a2p - (i <= nx - 2 ? a2 : T(0));
+    T ex = a.E[0][idx] + (fz3 + fy5);
+    T ey = a.E[1][idx] + (fz1 + fx4);
+    T ez = a.E[2][idx] + (fy0 + fx2);
+    if (sd.active) add_seed<T>(sd, i, j, k, ex, ey, ez);
+    a.E[0][idx] = ex;
+    a.E[1][idx] = ey;
+    a.E[2][idx] = ez;
+}
+
+// Seed only (before the first reverse step): one thread per patch cell.
+template <typename T>
+__global__ void k_adj_seed(int nx, int ny, int nz, T *E0, T *E1, T *E2, AdjSeed sd) {
+    const int64_t na = sd.a1 - sd.a0, nb = sd.b1 - sd.b0;
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= na * nb) return;
+    const int pa = sd.a0 + (int)(q / nb), pb = sd.b0 + (int)(q % nb);
+    int i, j, k;
+    if (sd.axis == 0) { i = sd.index; j = pa; k = pb; }
+    else if (sd.axis == 1) { i = pa; j = sd.index; k = pb; }
+    else { i = pa; j = pb; k = sd.index; }
+    const int64_t idx = ((int64_t)i * ny + j) * nz + k;
+    T ex = E0[idx], ey = E1[idx], ez = E2[idx];
+    add_seed<T>(sd, i, j, k, ex, ey, ez);
+    E0[idx] = ex;
+    E1[idx] = ey;
+    E2[idx] = ez;
+}
+
+// E over box [lo, hi) -> out[3][box cells].
+template <typename T>
+__global__ void k_capture(int ny, int nz, const T *E0, const T *E1, const T *E2, int3 lo,
+                          int3 ext, T *out) {
+    const int64_t nb = (int64_t)ext.x * ext.y * ext.z;
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 3 * nb) return;
+    const int c = (int)(q / nb);
+    const int64_t r = q - c * nb;
+    const int kk = (int)(r % ext.z);
+    const int64_t t = r / ext.z;
+    const int jj = (int)(t % ext.y), ii = (int)(t / ext.y);
+    const int64_t idx = ((int64_t)(lo.x + ii) * ny + (lo.y + jj)) * nz + (lo.z + kk);
+    const T *src = c == 0 ? E0 : (c == 1 ? E1 : E2);
+    out[q] = src[idx];
+}
+
+template <typename T>
+cudaError_t launch_adjoint_step(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjSeed &sd,
+                                cudaStream_t st) {
+    dim3 blk(ADJ_TK, ADJ_TJ, 1);
+    dim3 grd((a.nz + ADJ_TK - 1) / ADJ_TK, (a.ny + ADJ_TJ - 1) / ADJ_TJ, a.nx);
+    k_adj_H<T><<<grd, blk, 0, st>>>(a, gb);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_adj_E<T><<<grd, blk, 0, st>>>(a, sd);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_adjoint_seed(int nx, int ny, int nz, T *const E[3], const AdjSeed &sd,
+                                cudaStream_t st) {
+    const int64_t n = (int64_t)(sd.a1 - sd.a0) * (sd.b1 - sd.b0);
+    if (n <= 0) return cudaSuccess;
+    const int thr = 256;
+    k_adj_seed<T><<<(unsigned)((n + thr - 1) / thr), thr, 0, st>>>(nx, ny, nz, E[0], E[1], E[2],
+                                                                  sd);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_capture(int ny, int nz, const T *const E[3], const int lo[3], const int hi[3],
+                           T *out, cudaStream_t st) {
+    const int3 l = make_int3(lo[0], lo[1], lo[2]);
+    const int3 ext = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    const int64_t n = 3 * (int64_t)ext.x * ext.y * ext.z;
+    if (n <= 0) return cudaSuccess;
+    const int thr = 256;
+    k_capture<T><<<(unsigned)((n + thr - 1) / thr), thr, 0, st>>>(ny, nz, E[0], E[1], E[2], l,
+                                                                 ext, out);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_adjoint_step<float>(const AdjArgs<float> &, const AdjGrad<float> &,
+                                                const AdjSeed &, cudaStream_t);
+template cudaError_t launch_adjoint_step<double>(const AdjArgs<double> &,
+                                                 const AdjGrad<double> &, const AdjSeed &,
+                                                 cudaStream_t);
+template cudaError_t launch_adjoint_seed<float>(int, int, int, float *const[3], const AdjSeed &,
+                                                cudaStream_t);
+template cudaError_t launch_adjoint_seed<double>(int, int, int, double *const[3],
+                                                 const AdjSeed &, cudaStream_t);
+template cudaError_t launch_capture<float>(int, int, const float *const[3], const int[3],
+                                           const int[3], float *, cudaStream_t);
+template cudaError_t launch_capture<double>(int, int, const double *const[3], const int[3],
+                                            const int[3], double *, cudaStream_t);
+
+}  // namespace fdtd

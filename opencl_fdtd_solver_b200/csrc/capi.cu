@@ -9,6 +9,7 @@
 
 #include "../../include/fdtd_b200.h"
 #include "yee_launch.cuh"
+#include "adjoint.cuh"
 
 namespace fdtd {
 template <typename T>
@@ -190,6 +191,110 @@ int check_box(const fdtd_grid *g, const fdtd_box *b) {
     return FDTD_OK;
 }
 
+// ---- adjoint --------------------------------------------------------------
+int check_adjoint(const fdtd_grid *g, const fdtd_adjoint_fields *a) {
+    if (!a) return fail(FDTD_ERR_INVALID, "adjoint fields is NULL");
+    if (g->lossy)
+        return fail(FDTD_ERR_UNSUPPORTED, "the adjoint sweep needs a lossless grid (ca == 1)");
+    for (int c = 0; c < 3; ++c)
+        if (!a->E[c] || !a->H[c] || !a->ce[c])
+            return fail(FDTD_ERR_INVALID, "adjoint field/coefficient pointer %d is NULL", c);
+    if (g->npml > 0)
+        for (int q = 0; q < 6; ++q) {
+            if (!a->pe[q] || !a->pe_next[q] || !a->ph[q] || !a->ph_next[q])
+                return fail(FDTD_ERR_INVALID, "adjoint P stripe %d is NULL", q);
+            if (a->pe[q] == a->pe_next[q] || a->ph[q] == a->ph_next[q])
+                return fail(FDTD_ERR_INVALID, "adjoint P stripe %d: next must not alias", q);
+        }
+    return FDTD_OK;
+}
+
+int build_seed(const fdtd_grid *g, const fdtd_adjoint_seed *s, fdtd::AdjSeed &out) {
+    memset(&out, 0, sizeof(out));
+    if (!s) return FDTD_OK;
+    const int dims[3] = {g->nx, g->ny, g->nz};
+    if (s->axis < 0 || s->axis > 2) return fail(FDTD_ERR_INVALID, "seed axis %d", s->axis);
+    if (s->index < 0 || s->index >= dims[s->axis])
+        return fail(FDTD_ERR_INVALID, "seed plane index %d outside [0, %d)", s->index,
+                    dims[s->axis]);
+    const int da = s->axis == 0 ? dims[1] : dims[0];
+    const int db = s->axis == 2 ? dims[1] : dims[2];
+    if (s->a0 < 0 || s->a1 > da || s->a0 >= s->a1 || s->b0 < 0 || s->b1 > db || s->b0 >= s->b1)
+        return fail(FDTD_ERR_INVALID, "seed patch [%d,%d)x[%d,%d) is empty or outside the %dx%d plane",
+                    s->a0, s->a1, s->b0, s->b1, da, db);
+    if (s->comp_mask <= 0 || s->comp_mask > 7)
+        return fail(FDTD_ERR_INVALID, "seed comp_mask 0x%x (E components only)", s->comp_mask);
+    if (s->nfreq < 1 || s->nfreq > FDTD_MAX_FREQS)
+        return fail(FDTD_ERR_INVALID, "seed nfreq %d outside [1, %d]", s->nfreq, FDTD_MAX_FREQS);
+    if (!s->seed || !s->phase) return fail(FDTD_ERR_INVALID, "seed/phase is NULL");
+    out.active = 1;
+    out.axis = s->axis;
+    out.index = s->index;
+    out.a0 = s->a0;
+    out.a1 = s->a1;
+    out.b0 = s->b0;
+    out.b1 = s->b1;
+    out.comp_mask = s->comp_mask;
+    out.nfreq = s->nfreq;
+    out.seed = s->seed;
+    out.phase = s->phase;
+    return FDTD_OK;
+}
+
+int check_span(const fdtd_grid *g, const int32_t lo[3], const int32_t hi[3], const char *what) {
+    const int dims[3] = {g->nx, g->ny, g->nz};
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] < 0 || hi[a] > dims[a] || lo[a] >= hi[a])
+            return fail(FDTD_ERR_INVALID, "%s axis %d: [%d, %d) is empty or outside [0, %d)", what,
+                        a, lo[a], hi[a], dims[a]);
+    return FDTD_OK;
+}
+
+template <typename T>
+fdtd::AdjArgs<T> make_adj(const fdtd_grid *g, const fdtd_adjoint_fields *f, const fdtd_cpml *c) {
+    fdtd::AdjArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    a.nx = g->nx;
+    a.ny = g->ny;
+    a.nz = g->nz;
+    a.npml = g->npml;
+    a.dtm = (T)g->dtm;
+    for (int q = 0; q < 3; ++q) {
+        a.E[q] = (T *)f->E[q];
+        a.H[q] = (T *)f->H[q];
+        a.ce[q] = (const T *)f->ce[q];
+        a.cph.b[q] = (const T *)c->b_h[q];
+        a.cph.c[q] = (const T *)c->c_h[q];
+        a.cph.ik[q] = (const T *)c->ik_h[q];
+        a.cpe.b[q] = (const T *)c->b_e[q];
+        a.cpe.c[q] = (const T *)c->c_e[q];
+        a.cpe.ik[q] = (const T *)c->ik_e[q];
+    }
+    for (int q = 0; q < 6; ++q) {
+        a.pe[q] = (const T *)f->pe[q];
+        a.pe_next[q] = (T *)f->pe_next[q];
+        a.ph[q] = (const T *)f->ph[q];
+        a.ph_next[q] = (T *)f->ph_next[q];
+    }
+    return a;
+}
+
+template <typename T>
+fdtd::AdjGrad<T> make_grad(const fdtd_grad_box *gb) {
+    fdtd::AdjGrad<T> r;
+    memset(&r, 0, sizeof(r));
+    if (!gb) return r;
+    r.active = 1;
+    for (int q = 0; q < 3; ++q) {
+        r.lo[q] = gb->lo[q];
+        r.hi[q] = gb->hi[q];
+    }
+    r.e_next = (const T *)gb->e_next;
+    r.e_prev = (const T *)gb->e_prev;
+    r.g = gb->g;
+    return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -333,6 +438,67 @@ int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl,
     return cuda_status(fdtd::launch_farfield(*box, acc, fi, dl, k_wave, eta0, obs_xyz, n_obs,
                                              nl_scratch, eh, (cudaStream_t)stream),
                        "farfield");
+}
+
+int fdtd_capture_box(const fdtd_grid *g, const void *const E[3], const int32_t lo[3],
+                     const int32_t hi[3], void *out, void *stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!E || !E[0] || !E[1] || !E[2] || !out || !lo || !hi)
+        return fail(FDTD_ERR_INVALID, "NULL buffer");
+    if ((rc = check_span(g, lo, hi, "capture box"))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_capture<float>(g->ny, g->nz, (const float *const *)E, lo,
+                                                       hi, (float *)out, st),
+                           "capture_box");
+    return cuda_status(fdtd::launch_capture<double>(g->ny, g->nz, (const double *const *)E, lo,
+                                                    hi, (double *)out, st),
+                       "capture_box");
+}
+
+int fdtd_adjoint_seed_add(const fdtd_grid *g, void *const Ebar[3], const fdtd_adjoint_seed *seed,
+                          void *stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!Ebar || !Ebar[0] || !Ebar[1] || !Ebar[2] || !seed)
+        return fail(FDTD_ERR_INVALID, "NULL buffer");
+    fdtd::AdjSeed sd;
+    if ((rc = build_seed(g, seed, sd))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_adjoint_seed<float>(g->nx, g->ny, g->nz,
+                                                            (float *const *)Ebar, sd, st),
+                           "adjoint_seed_add");
+    return cuda_status(fdtd::launch_adjoint_seed<double>(g->nx, g->ny, g->nz,
+                                                         (double *const *)Ebar, sd, st),
+                       "adjoint_seed_add");
+}
+
+int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fdtd_cpml *c,
+                      const fdtd_grad_box *gb, const fdtd_adjoint_seed *next_seed,
+                      void *stream) {
+    int rc;
+    if ((rc = check_grid(g)) || (rc = check_adjoint(g, a))) return rc;
+    if (!c) return fail(FDTD_ERR_INVALID, "cpml is NULL");
+    for (int q = 0; q < 3; ++q)
+        if (!c->b_h[q] || !c->c_h[q] || !c->ik_h[q] || !c->b_e[q] || !c->c_e[q] || !c->ik_e[q])
+            return fail(FDTD_ERR_INVALID, "CPML profile pointer for axis %d is NULL", q);
+    if (gb) {
+        if ((rc = check_span(g, gb->lo, gb->hi, "gradient box"))) return rc;
+        if (!gb->e_next || !gb->e_prev || !gb->g)
+            return fail(FDTD_ERR_INVALID, "gradient box buffer is NULL");
+    }
+    fdtd::AdjSeed sd;
+    if ((rc = build_seed(g, next_seed, sd))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g->dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_adjoint_step<float>(make_adj<float>(g, a, c),
+                                                            make_grad<float>(gb), sd, st),
+                           "adjoint_step");
+    return cuda_status(fdtd::launch_adjoint_step<double>(make_adj<double>(g, a, c),
+                                                         make_grad<double>(gb), sd, st),
+                       "adjoint_step");
 }
 
 }  // extern "C"

@@ -248,6 +248,20 @@ class CUDAFDTD(SourceMonitorMixin):
         self._refresh_structs()
 
     def _refresh_structs(self):
+        self._fields_by_parity = {}
+        self._build_fields()
+        cp = capi.Cpml.from_buffer_copy(self._cpml_base)
+        for q in range(6):
+            cp.psi_h[q] = self._psi_h[q].data_ptr()
+            cp.psi_e[q] = self._psi_e[q].data_ptr()
+        self._cpml = cp
+        self._grid.lossy = 1 if self.lossy else 0
+
+    def _build_fields(self):
+        cached = self._fields_by_parity.get(self._parity)
+        if cached is not None:
+            self._fields = cached
+            return
         f = capi.Fields()
         for a in range(3):
             f.E[a] = self._E[a].data_ptr()
@@ -259,12 +273,7 @@ class CUDAFDTD(SourceMonitorMixin):
                 f.E_next[a] = self._En[a].data_ptr()
                 f.H_next[a] = self._Hn[a].data_ptr()
         self._fields = f
-        cp = capi.Cpml.from_buffer_copy(self._cpml_base)
-        for q in range(6):
-            cp.psi_h[q] = self._psi_h[q].data_ptr()
-            cp.psi_e[q] = self._psi_e[q].data_ptr()
-        self._cpml = cp
-        self._grid.lossy = 1 if self.lossy else 0
+        self._fields_by_parity[self._parity] = f
 
     # -------------------------------------------------------------- materials
     def set_epsilon(self, eps_array, sigma_array=None):
@@ -411,7 +420,7 @@ class CUDAFDTD(SourceMonitorMixin):
         self._E, self._En = self._En, self._E
         self._H, self._Hn = self._Hn, self._H
         self._parity ^= 1
-        self._refresh_structs()
+        self._build_fields()
 
     def run(self, n_steps, progress_every=0):
         """Run ``n_steps`` steps; log progress at INFO every ``progress_every`` steps."""
@@ -422,6 +431,40 @@ class CUDAFDTD(SourceMonitorMixin):
 
     def synchronize(self):
         self.queue.synchronize()
+
+    # ------------------------------------------------------ state snapshots
+    def _state_tensors(self):
+        """The tensors that carry the time-stepping state: E, H, ψ_H, ψ_E."""
+        return list(self._E) + list(self._H) + list(self._psi_h) + list(self._psi_e)
+
+    def save_state(self):
+        """Device copy of the full time-stepping state (fields, ψ stripes, t, step_num)."""
+        torch = _torch()
+        self._materialize()
+        with torch.cuda.stream(self.queue):
+            tensors = [t.clone() for t in self._state_tensors()]
+        return {"tensors": tensors, "t": self.t, "step_num": self.step_num}
+
+    def load_state(self, state):
+        """Restore a state taken by :meth:`save_state` on this engine."""
+        torch = _torch()
+        cur = self._state_tensors()
+        if len(cur) != len(state["tensors"]):
+            raise ValueError("state was saved from a different engine layout")
+        with torch.cuda.stream(self.queue):
+            for dst, src in zip(cur, state["tensors"]):
+                dst.copy_(src)
+        self.t = float(state["t"])
+        self.step_num = int(state["step_num"])
+
+    def reset_state(self):
+        """Zero the fields and ψ stripes and rewind to t = 0 (coefficients kept)."""
+        torch = _torch()
+        with torch.cuda.stream(self.queue):
+            for t in self._state_tensors():
+                t.zero_()
+        self.t = 0.0
+        self.step_num = 0
 
     # ----------------------------------------------------------- field access
     def field_tensor(self, name):

@@ -42,7 +42,9 @@ def test_library_exports_every_declared_symbol():
 def test_ctypes_structs_match_c_header(tmp_path):
     """sizeof/offsetof of every ABI struct, from gcc on the header, equal ctypes'."""
     structs = {"fdtd_grid": capi.Grid, "fdtd_fields": capi.Fields, "fdtd_cpml": capi.Cpml,
-               "fdtd_source": capi.Source, "fdtd_plane_dft": capi.PlaneDft, "fdtd_box": capi.Box}
+               "fdtd_source": capi.Source, "fdtd_plane_dft": capi.PlaneDft, "fdtd_box": capi.Box,
+               "fdtd_adjoint_fields": capi.AdjointFields, "fdtd_adjoint_seed": capi.AdjointSeed,
+               "fdtd_grad_box": capi.GradBox}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fdtd_b200.h"',
              'int main(void) {']
     for cname, py in structs.items():
