@@ -15,6 +15,11 @@ independent replica of the workload (the path is one grid per GPU here), timing
 is the max over ranks, and ``value`` is the total cell updates of all ranks per
 second ("scaling": "weak").
 
+The same line carries ``adjoint``: the ε-gradient leg at 160×160×96 FP32 (npml 12,
+96×96×16 design box, Jx sheet at 30 GHz, 3000 steps, checkpoints every 100 steps,
+objective Σ|Ex(30 GHz)|² over a 32×32 patch): ``t_grad / t_forward`` by CUDA events,
+and the gradient against central differences (h = 1e-3) at 16 seeded voxels in FP64.
+
 ``--impl reference`` times the reference's own Yee/source kernels
 (``opencl_fdtd_solver/kernels/yee_update.cl``, ``sources.cl``) compiled as C with
 OpenMP on all host cores (``oracle/_ref``; the C restatement in ``oracle/`` when
@@ -255,37 +260,51 @@ def run_reference_arm(args, rank, world):
     return line
 
 
-def time_steps(g, k, event_pairs=True):
-    """Device time (ms) of k steps on the engine's stream, bracketed by events."""
+def interior_alg_bytes(shape, npml, item=4):
+    """Algorithmic bytes of one launch of the interior single-pass kernel: for every
+    cell of the H box [npml, N-npml)^3 one read of E, H and ce and one write of E
+    and H (15 arrays x item), with no ψ and no DFT (those run in the shell and
+    plane-DFT kernels)."""
+    n = 1
+    for d in shape:
+        n *= max(0, d - 2 * npml)
+    return 15 * item * n
+
+
+def run_steps_timed(g, k):
+    """Device time (ms) of k steps on the engine's stream (events on that stream),
+    the library's per-launch times over the same steps, and its launch count."""
+    import ctypes
+
     import torch
 
+    from opencl_fdtd_solver_b200 import _capi as capi
+
+    lib = capi.lib()
     st = g.queue
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
-    per = []
     torch.cuda.synchronize()
+    n0 = lib.fdtd_launch_count()
+    capi.run("fdtd_profile_steps", 1)
     start.record(st)
-    evs = []
     for _ in range(k):
-        if event_pairs:
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(st)
         g.step()
-        if event_pairs:
-            b.record(st)
-            evs.append((a, b))
     end.record(st)
     torch.cuda.synchronize()
-    total = start.elapsed_time(end)
-    per = [a.elapsed_time(b) for a, b in evs]
-    return total, per
+    capi.run("fdtd_profile_steps", 0)
+    launches = lib.fdtd_launch_count() - n0
+    ms = (ctypes.c_double * 4)()
+    nsteps = ctypes.c_int32()
+    capi.run("fdtd_profile_read", ms, ctypes.byref(nsteps))
+    per_kernel = {name: ms[i] / max(1, nsteps.value)
+                  for i, name in enumerate(("k_shell_H", "k_interior", "k_plane_dft_box",
+                                            "k_shell_E"))}
+    return start.elapsed_time(end), per_kernel, launches
 
 
 def run_b200_arm(args, rank, world, local):
     import torch
-
-    from opencl_fdtd_solver_b200 import CUDAFDTD
 
     size, npml = args.size, args.npml
     shape = (size, size, size)
@@ -298,35 +317,40 @@ def run_b200_arm(args, rank, world, local):
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        total_ms, per = time_steps(g, args.steps)
+        total_ms, per_kernel, launches = run_steps_timed(g, args.steps)
     total_ms = reduce_max(total_ms, world)
     clocks = clk.summary()
     ms_per_step = total_ms / args.steps
     value = world * cells * args.steps / (total_ms / 1e3) / 1e6
     fused = g._fused_enabled
-    launches_per_step = 1 if fused else 2
 
-    # roofline of the dominant kernel (the fused step: one launch per step)
     item = 4
-    bpc = alg_bytes_per_cell(shape, npml, item, ((2, 1, len(FREQS)),))
-    per_launch_ms = statistics.mean(per)
-    achieved = bpc * cells / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm()
+    bpc = alg_bytes_per_cell(shape, npml, item, ((2, 1, len(FREQS)),))
+    step_achieved = bpc * cells / (ms_per_step / 1e3) / 1e9
+    if fused and per_kernel["k_interior"] > 0:
+        # dominant kernel: the interior single-pass kernel (largest share of the step)
+        k_ms = per_kernel["k_interior"]
+        k_bytes = interior_alg_bytes(shape, npml, item)
+        kname = "k_interior"
+    else:
+        kname, k_ms, k_bytes = "step (split kernels)", ms_per_step, bpc * cells
+    achieved = k_bytes / (k_ms / 1e3) / 1e9
     traffic = None
     tp = ROOT / "profiles" / "yee_step_traffic.json"
     if tp.exists():
         try:
             tj = json.loads(tp.read_text())
-            if tj.get("size") == size and tj.get("fused") == fused:
+            if tj.get("size") == size and tj.get("npml") == npml and tj.get("kernel") == kname:
                 traffic = tj.get("bytes_per_launch")
         except Exception:
             traffic = None
-
-    # end to end through the public API with host buffers: ε upload (host → ce on
-    # device), K steps with the Python source callback, DFT plane + one field
-    # plane read back to the host
     del g, mon
     torch.cuda.empty_cache()
+
+    # end to end through the public API with host buffers: a new engine, εr
+    # uploaded from the host (coefficients built on the device), K steps with the
+    # Python source callback, the DFT plane and one field plane read back
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -343,12 +367,16 @@ def run_b200_arm(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_wall = time.perf_counter() - t0
     e2e_dev_ms = reduce_max(ev0.elapsed_time(ev1), world)
-    e2e_s = max(e2e_dev_ms / 1e3, 0.0)
-    e2e_value = world * cells * args.steps / e2e_s / 1e6
-    h2d = 3 * cells * item  # ce arrays built from the host ε
+    e2e_value = world * cells * args.steps / (e2e_dev_ms / 1e3) / 1e6
+    h2d = eps.nbytes  # εr; the coefficients are built on the device
     d2h = dft.nbytes + plane.nbytes
     del g2, mon2
     torch.cuda.empty_cache()
+
+    adjoint = None
+    if not args.no_adjoint:
+        barrier(world)
+        adjoint = run_adjoint_leg(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -369,18 +397,158 @@ def run_b200_arm(args, rank, world, local):
                    "eps_seed": 1234, "fused_step": fused,
                    "l2": "inputs (~9 GB/step) exceed L2; no flush",
                    "parallelism": f"replicas{world}"},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": peak_kind, "alg_bytes_per_cell": round(bpc, 3)},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "alg_bytes_per_launch": int(k_bytes),
+                     "ms_per_launch": round(k_ms, 4)},
+        "step_roofline": {"alg_bytes_per_cell": round(bpc, 3),
+                          "achieved": round(step_achieved, 1),
+                          "frac": round(step_achieved / peak, 4),
+                          "ms_per_launch": {k: round(v, 4) for k, v in per_kernel.items()}},
         "e2e": {"value": round(e2e_value, 1), "unit": "Mcell/s",
                 "h2d_bytes_per_step": int(h2d / args.steps),
                 "d2h_bytes_per_step": int(d2h / args.steps),
                 "wall_s": round(e2e_wall, 3)},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     return line
+
+
+# --------------------------------------------------------------- adjoint leg
+ADJ_SHAPE = (160, 160, 96)
+ADJ_NPML = 12
+ADJ_DESIGN = ((32, 128), (32, 128), (40, 56))
+ADJ_SHEET = dict(z=24, i0=12, i1=148, j0=12, j1=148)
+ADJ_PLANE = 72
+ADJ_PATCH = ((64, 96), (64, 96))
+ADJ_FREQ = 30e9
+ADJ_STEPS = 3000
+ADJ_K = 100
+
+
+def gaussian_sine(t, f0=30e9, fwidth=10e9):
+    t0 = 5.0 / (np.pi * fwidth)
+    sigma = 1.0 / (np.pi * fwidth)
+    return float(np.exp(-0.5 * ((t - t0) / sigma) ** 2) * np.sin(2 * np.pi * f0 * t))
+
+
+def design_eps(seed=2024, corr=6.0):
+    """εr = 1 + 3·sigmoid(g) over the design box, g a seeded Gaussian random field
+    (white noise smoothed by a Gaussian of σ = ``corr`` cells, periodic, unit variance)."""
+    dims = tuple(hi - lo for lo, hi in ADJ_DESIGN)
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(dims)
+    k = [np.fft.fftfreq(n) for n in dims]
+    kk = sum(np.meshgrid(*[(2 * np.pi * v) ** 2 for v in k], indexing="ij"))
+    g = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-0.5 * corr**2 * kk)))
+    g = (g - g.mean()) / g.std()
+    return 1.0 + 3.0 / (1.0 + np.exp(-g))
+
+
+def adjoint_problem(dtype):
+    from opencl_fdtd_solver_b200 import CUDAFDTD, DFTObjective, EpsilonAdjoint
+
+    fd = CUDAFDTD(ADJ_SHAPE, 1e-3, npml=ADJ_NPML, dtype=dtype)
+    s = ADJ_SHEET
+    fd.add_source(lambda f: f.add_source_Jx(s["z"], gaussian_sine(f.t), s["i0"], s["i1"],
+                                            s["j0"], s["j1"], rim_taper=True))
+    obj = DFTObjective("z", ADJ_PLANE, ADJ_PATCH, [ADJ_FREQ], ("Ex",))
+    return EpsilonAdjoint(fd, ADJ_DESIGN, ADJ_STEPS, obj, checkpoint_every=ADJ_K)
+
+
+def plain_forward(adj, eps_d):
+    """One forward solve without checkpoints: set εr, run N steps with the DFT, read J."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import CUDAPlaneDFTMonitor
+
+    fd, o = adj.fdtd, adj.objective
+    fd.set_epsilon(adj._eps_full(eps_d))
+    fd.reset_state()
+    saved = fd._monitors
+    fd._monitors = []
+    try:
+        mon = CUDAPlaneDFTMonitor(fd, o.axis, o.index, o.freqs, o.components)
+        fd.run(adj.n_steps)
+    finally:
+        fd._monitors = saved
+    (a0, a1), (b0, b1) = o.patch
+    D = torch.view_as_complex(mon.acc)[:, :, a0:a1, b0:b1]
+    return float(o.fn(D))
+
+
+def timed(fn, stream):
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def run_adjoint_leg(args):
+    """t_grad / t_forward at the adjoint configuration (FP32), and the gradient
+    checked against central differences (h = 1e-3) at 16 seeded voxels in FP64."""
+    import torch
+
+    eps_d = design_eps()
+    adj = adjoint_problem(np.float32)
+    st = adj.fdtd.queue
+    adj.value_and_grad(eps_d)  # warm-up
+    plain_forward(adj, eps_d)
+    t_fwd = min(timed(lambda: plain_forward(adj, eps_d), st)[0] for _ in range(3))
+    t_grad, (J32, g32) = min((timed(lambda: adj.value_and_grad(eps_d), st) for _ in range(3)),
+                             key=lambda r: r[0])
+    del adj
+    torch.cuda.empty_cache()
+    adj64 = adjoint_problem(np.float64)
+    t64, (J64, g64) = timed(lambda: adj64.value_and_grad(eps_d), adj64.fdtd.queue)
+    rng = np.random.default_rng(16)
+    dims = g64.shape
+    voxels = [tuple(int(rng.integers(0, d)) for d in dims) for _ in range(16)]
+    h = 1e-3
+    fd_g = []
+    for v in voxels:
+        ep = eps_d.copy()
+        ep[v] += h
+        jp = adj64.forward(ep)
+        ep[v] -= 2 * h
+        jm = adj64.forward(ep)
+        fd_g.append((jp - jm) / (2 * h))
+    fd_g = np.array(fd_g)
+    ad64 = np.array([g64[v] for v in voxels])
+    ad32 = np.array([g32[v] for v in voxels])
+    n_design = int(np.prod(dims))
+    del adj64
+    torch.cuda.empty_cache()
+    return {
+        "workload": (f"adjoint_{ADJ_SHAPE[0]}x{ADJ_SHAPE[1]}x{ADJ_SHAPE[2]}_npml{ADJ_NPML}_"
+                     f"design{dims[0]}x{dims[1]}x{dims[2]}_jx_sheet_30GHz_{ADJ_STEPS}steps_"
+                     f"patch32x32_K{ADJ_K}"),
+        "t_forward_ms": round(t_fwd, 2),
+        "t_grad_ms": round(t_grad, 2),
+        "grad_cost_forward_solves": round(t_grad / t_fwd, 3),
+        "target_forward_solves": 4,
+        "fd_gradient_cost_forward_solves": n_design + 1,
+        "fd_gradient_ms_extrapolated": round((n_design + 1) * t_fwd, 1),
+        "speedup_vs_fd_gradient": round((n_design + 1) * t_fwd / t_grad, 1),
+        "fd_check": {"voxels": len(voxels), "h": h, "dtype": "f64",
+                     "rel_err": float(np.linalg.norm(ad64 - fd_g) / np.linalg.norm(fd_g)),
+                     "rel_err_fp32_adjoint_vs_fd": float(np.linalg.norm(ad32 - fd_g)
+                                                         / np.linalg.norm(fd_g))},
+        "fp32_vs_fp64_grad_rel_err": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+        "J_fp32": J32, "J_fp64": J64, "t_grad_fp64_ms": round(t64, 2),
+        "design_eps": "1 + 3 sigmoid(GRF), sigma 6 cells, seed 2024",
+    }
 
 
 def main(argv=None):
@@ -395,6 +563,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="CPU-baseline sample length beside the GPU arm")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint-gradient leg (t_grad / t_forward, FD check)")
     ap.add_argument("--cpu-budget", type=float, default=150.0,
                     help="time budget of the --impl reference arm's timed steps")
     args = ap.parse_args(argv)

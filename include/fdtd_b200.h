@@ -249,7 +249,34 @@ int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fd
                       const fdtd_grad_box *gb, const fdtd_adjoint_seed *next_seed,
                       void *stream);
 
+/* ---- materials ----------------------------------------------------------- */
+
+/* Yee-edge coefficients from cell-centred εr (and conductivity σ in S/m, may
+ * be NULL) computed on the device: ce = (dt/eps0)/ε_edge, or with σ the lossy
+ * ca = (1-loss)/(1+loss) and cb = (dt/(eps0 ε_edge))/(1+loss) with
+ * loss = (σ_edge dt)/((2 eps0) ε_edge), where ε_edge (σ_edge) is the mean of
+ * the two cells sharing the edge and the last plane keeps the cell value.
+ * float64 arithmetic in the order of materials.py:28-88, rounded once to the
+ * grid dtype, so the result equals set_epsilon's host math (engine.py:212-254)
+ * bit for bit.  eps/sigma: nx*ny*nz values of eps_dtype in C order (device).
+ * ce receives cb when sigma is given; ca is written only then. */
+int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int32_t eps_dtype,
+                     double dt, double eps0, void *const ce[3], void *const ca[3], void *stream);
+
 /* ---- diagnostics --------------------------------------------------------- */
+
+/* Device time of each launch of fdtd_step, for measurement.  enable != 0 clears
+ * the sums and records CUDA events around every launch of each following
+ * fdtd_step on its stream; enable == 0 stops recording.  fdtd_profile_read
+ * waits for the recorded events and returns the summed milliseconds per
+ * launch, [0] CPML-shell H, [1] interior single-pass kernel, [2] plane DFT of
+ * the interior, [3] CPML-shell E (with sources and DFTs), and the number of
+ * steps recorded.  No reference counterpart. */
+int fdtd_profile_steps(int32_t enable);
+int fdtd_profile_read(double ms[4], int32_t *nsteps);
+
+/* Number of kernel launches this library has issued since it was loaded. */
+int64_t fdtd_launch_count(void);
 
 /* Message for the last non-OK status returned on this host thread. */
 const char *fdtd_last_error(void);

@@ -10,7 +10,7 @@ engine fails loudly.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_void_p
+from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libfdtd_b200.so"
@@ -104,6 +104,11 @@ SIGNATURES = {
                                         c_void_p]),
     "fdtd_adjoint_step": (c_int32, [POINTER(Grid), POINTER(AdjointFields), POINTER(Cpml),
                                     POINTER(GradBox), POINTER(AdjointSeed), c_void_p]),
+    "fdtd_set_epsilon": (c_int32, [POINTER(Grid), c_void_p, c_void_p, c_int32, c_double,
+                                   c_double, POINTER(c_void_p), POINTER(c_void_p), c_void_p]),
+    "fdtd_profile_steps": (c_int32, [c_int32]),
+    "fdtd_profile_read": (c_int32, [POINTER(c_double), POINTER(c_int32)]),
+    "fdtd_launch_count": (c_int64, []),
     "fdtd_last_error": (c_char_p, []),
     "fdtd_device_status": (c_int32, [POINTER(c_int32), c_int32]),
     "fdtd_version": (c_char_p, []),

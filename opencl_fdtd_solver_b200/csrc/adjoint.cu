@@ -32,6 +32,7 @@
 
 #include <cstdint>
 
+#include "launch_count.cuh"
 #include "../../include/fdtd_b200.h"
 #include "adjoint.cuh"
 
@@ -262,9 +263,11 @@ cudaError_t launch_adjoint_step(const AdjArgs<T> &a, const AdjGrad<T> &gb, const
     dim3 blk(ADJ_TK, ADJ_TJ, 1);
     dim3 grd((a.nz + ADJ_TK - 1) / ADJ_TK, (a.ny + ADJ_TJ - 1) / ADJ_TJ, a.nx);
     k_adj_H<T><<<grd, blk, 0, st>>>(a, gb);
+    count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_adj_E<T><<<grd, blk, 0, st>>>(a, sd);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -276,6 +279,7 @@ cudaError_t launch_adjoint_seed(int nx, int ny, int nz, T *const E[3], const Adj
     const int thr = 256;
     k_adj_seed<T><<<(unsigned)((n + thr - 1) / thr), thr, 0, st>>>(nx, ny, nz, E[0], E[1], E[2],
                                                                   sd);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -289,6 +293,7 @@ cudaError_t launch_capture(int ny, int nz, const T *const E[3], const int lo[3],
     const int thr = 256;
     k_capture<T><<<(unsigned)((n + thr - 1) / thr), thr, 0, st>>>(ny, nz, E[0], E[1], E[2], l,
                                                                  ext, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 

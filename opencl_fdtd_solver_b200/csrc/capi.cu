@@ -2,6 +2,7 @@
 // argument validation, dtype dispatch, status codes and error messages.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +24,18 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
                             double k_wave, double eta0, const double *obs, int n_obs,
                             double *nl, double *eh, cudaStream_t st);
 int read_fused_error(int reset);
+void profile_enable(bool on);
+cudaError_t profile_read(double ms[4], int *steps);
+struct MatScalars {
+    double scale, dt, two_eps0, eps0;
+};
+template <typename T, typename S>
+cudaError_t launch_edge_coeffs(int nx, int ny, int nz, const S *eps, const S *sigma,
+                               const MatScalars &m, T *const ce[3], T *const ca[3],
+                               cudaStream_t st);
+
+std::atomic<long long> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 int noalloc_rel_max_face();
 cudaError_t launch_rel_change_noalloc(const double *cur, const double *prev, int n, int nfreq,
                                       int fi, double *out2, cudaStream_t st);
@@ -499,6 +512,65 @@ int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fd
     return cuda_status(fdtd::launch_adjoint_step<double>(make_adj<double>(g, a, c),
                                                          make_grad<double>(gb), sd, st),
                        "adjoint_step");
+}
+
+int fdtd_profile_steps(int32_t enable) {
+    fdtd::profile_enable(enable != 0);
+    return FDTD_OK;
+}
+
+int fdtd_profile_read(double ms[4], int32_t *nsteps) {
+    if (!ms || !nsteps) return fail(FDTD_ERR_INVALID, "NULL output");
+    int n = 0;
+    cudaError_t e = fdtd::profile_read(ms, &n);
+    *nsteps = n;
+    return cuda_status(e, "profile_read");
+}
+
+int64_t fdtd_launch_count(void) { return fdtd::g_launches.load(std::memory_order_relaxed); }
+
+int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int32_t eps_dtype,
+                     double dt, double eps0, void *const ce[3], void *const ca[3], void *stream) {
+    int rc;
+    if ((rc = check_grid(g))) return rc;
+    if (!eps || !ce || !ce[0] || !ce[1] || !ce[2]) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    if (sigma && (!ca || !ca[0] || !ca[1] || !ca[2]))
+        return fail(FDTD_ERR_INVALID, "sigma given without ca outputs");
+    if (eps_dtype != FDTD_F32 && eps_dtype != FDTD_F64)
+        return fail(FDTD_ERR_INVALID, "eps_dtype must be FDTD_F32 or FDTD_F64, got %d", eps_dtype);
+    if (!(dt > 0) || !(eps0 > 0)) return fail(FDTD_ERR_INVALID, "dt and eps0 must be positive");
+    fdtd::MatScalars m;
+    m.scale = dt / eps0;
+    m.dt = dt;
+    m.two_eps0 = 2.0 * eps0;
+    m.eps0 = eps0;
+    cudaStream_t st = (cudaStream_t)stream;
+    void *const nul[3] = {nullptr, nullptr, nullptr};
+    void *const *cav = sigma ? ca : nul;
+    cudaError_t e;
+    if (g->dtype == FDTD_F32) {
+        if (eps_dtype == FDTD_F32)
+            e = fdtd::launch_edge_coeffs<float, float>(g->nx, g->ny, g->nz, (const float *)eps,
+                                                       (const float *)sigma, m, (float *const *)ce,
+                                                       (float *const *)cav, st);
+        else
+            e = fdtd::launch_edge_coeffs<float, double>(g->nx, g->ny, g->nz, (const double *)eps,
+                                                        (const double *)sigma, m,
+                                                        (float *const *)ce, (float *const *)cav, st);
+    } else {
+        if (eps_dtype == FDTD_F32)
+            e = fdtd::launch_edge_coeffs<double, float>(g->nx, g->ny, g->nz, (const float *)eps,
+                                                        (const float *)sigma, m,
+                                                        (double *const *)ce, (double *const *)cav,
+                                                        st);
+        else
+            e = fdtd::launch_edge_coeffs<double, double>(g->nx, g->ny, g->nz,
+                                                         (const double *)eps,
+                                                         (const double *)sigma, m,
+                                                         (double *const *)ce,
+                                                         (double *const *)cav, st);
+    }
+    return cuda_status(e, "set_epsilon");
 }
 
 }  // extern "C"

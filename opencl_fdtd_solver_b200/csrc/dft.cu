@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "launch_count.cuh"
 #include "../../include/fdtd_b200.h"
 
 namespace fdtd {
@@ -295,6 +296,7 @@ cudaError_t launch_dft_faces(int nx, int ny, int nz, const T *const E[3], const 
     const int thr = 128;
     k_dft_faces<T><<<(b.n_face + thr - 1) / thr, thr, 0, st>>>(nx, ny, nz, E[0], E[1], E[2],
                                                                H[0], H[1], H[2], b, acc, phase);
+    count_launches(1);
     return cudaGetLastError();
 }
 template cudaError_t launch_dft_faces<float>(int, int, int, const float *const[3],
@@ -315,7 +317,9 @@ cudaError_t launch_rel_change(const double *cur, const double *prev, int n, int 
     k_rel_partial<<<nb, REL_THREADS, 0, st>>>(reinterpret_cast<const double2 *>(cur),
                                               reinterpret_cast<const double2 *>(prev), n, nfreq,
                                               fi, scratch);
+    count_launches(1);
     k_rel_final<<<1, REL_THREADS, 0, st>>>(scratch, nb, out2);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -366,7 +370,9 @@ cudaError_t launch_rel_change_noalloc(const double *cur, const double *prev, int
     k_rel_partial<<<nb, REL_THREADS, 0, st>>>(reinterpret_cast<const double2 *>(cur),
                                               reinterpret_cast<const double2 *>(prev), n, nfreq,
                                               fi, scratch);
+    count_launches(1);
     k_rel_final<<<1, REL_THREADS, 0, st>>>(scratch, nb, out2);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -376,9 +382,11 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
     k_farfield_nl<<<n_obs, FF_THREADS, 0, st>>>(b, reinterpret_cast<const double2 *>(acc), fi,
                                                 dl, k_wave, obs, n_obs,
                                                 reinterpret_cast<double2 *>(nl));
+    count_launches(1);
     k_farfield_eh<<<(n_obs + 127) / 128, 128, 0, st>>>(reinterpret_cast<const double2 *>(nl),
                                                        obs, n_obs, k_wave, eta0,
                                                        reinterpret_cast<double2 *>(eh));
+    count_launches(1);
     return cudaGetLastError();
 }
 

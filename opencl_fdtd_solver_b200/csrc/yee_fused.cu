@@ -37,6 +37,9 @@
 // flag, drains its outstanding copies (bounded again) and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <array>
+#include <vector>
 #include <cudaTypedefs.h>
 
 #include <cmath>
@@ -46,6 +49,7 @@
 #include <mutex>
 #include <unordered_map>
 
+#include "launch_count.cuh"
 #include "yee_launch.cuh"
 
 namespace fdtd {
@@ -598,6 +602,7 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
         if (e != cudaSuccess) return e;                                                        \
         k_interior<T, LS, NS><<<grid, NTHREADS, smem, st>>>(maps, a, bx, src);                 \
+        count_launches(1);                                                                     \
     } while (0)
     if (a.lossy) {
         if (nstage == 3) FDTD_LAUNCH_INTERIOR(true, 3);
@@ -611,6 +616,71 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
 }
 
 }  // namespace
+
+// ---- per-launch timing of the step (diagnostics) ---------------------------
+namespace {
+struct StepProfiler {
+    std::mutex mu;
+    bool on = false;
+    std::vector<std::array<cudaEvent_t, 5>> pending;
+    double ms[4] = {0.0, 0.0, 0.0, 0.0};
+    int steps = 0;
+};
+StepProfiler g_prof;
+
+// Waits for the recorded steps, adds their launch times, releases the events.
+cudaError_t prof_flush_locked() {
+    cudaError_t err = cudaSuccess;
+    for (auto &ev : g_prof.pending) {
+        cudaError_t e = cudaEventSynchronize(ev[4]);
+        for (int s = 0; s < 4 && e == cudaSuccess; ++s) {
+            float t = 0.f;
+            e = cudaEventElapsedTime(&t, ev[s], ev[s + 1]);
+            g_prof.ms[s] += t;
+        }
+        if (e != cudaSuccess) err = e;
+        for (cudaEvent_t x : ev) cudaEventDestroy(x);
+        ++g_prof.steps;
+    }
+    g_prof.pending.clear();
+    return err;
+}
+
+bool prof_begin(std::array<cudaEvent_t, 5> &ev) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    if (!g_prof.on) return false;
+    for (int s = 0; s < 5; ++s)
+        if (cudaEventCreate(&ev[s]) != cudaSuccess) {
+            for (int q = 0; q < s; ++q) cudaEventDestroy(ev[q]);
+            return false;
+        }
+    return true;
+}
+
+void prof_end(const std::array<cudaEvent_t, 5> &ev) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    g_prof.pending.push_back(ev);
+    if (g_prof.pending.size() >= 2048) prof_flush_locked();
+}
+}  // namespace
+
+void profile_enable(bool on) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    if (on) {
+        prof_flush_locked();
+        for (double &m : g_prof.ms) m = 0.0;
+        g_prof.steps = 0;
+    }
+    g_prof.on = on;
+}
+
+cudaError_t profile_read(double ms[4], int *steps) {
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    cudaError_t e = prof_flush_locked();
+    for (int s = 0; s < 4; ++s) ms[s] = g_prof.ms[s];
+    *steps = g_prof.steps;
+    return e;
+}
 
 template <typename T>
 cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const PlaneList &pl,
@@ -636,18 +706,22 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
         ebox.lo[d] = use_interior ? a.npml + 1 : 0;
         ebox.hi[d] = use_interior ? n[d] - a.npml : 0;
     }
+    std::array<cudaEvent_t, 5> ev;
+    const bool prof = prof_begin(ev);
+    if (prof) cudaEventRecord(ev[0], st);
     cudaError_t e = launch_shell_H<T>(a, hbox, st);
-    if (e != cudaSuccess) return e;
-    if (use_interior) {
-        e = launch_interior<T>(a, maps, hbox, src, st);
-        if (e != cudaSuccess) return e;
-        // plane DFTs of the cells the interior kernel updated
-        if (pl.n) {
-            e = launch_plane_dft_box<T>(a, ebox, pl, st);
-            if (e != cudaSuccess) return e;
-        }
+    if (prof) cudaEventRecord(ev[1], st);
+    if (e == cudaSuccess && use_interior) e = launch_interior<T>(a, maps, hbox, src, st);
+    if (prof) cudaEventRecord(ev[2], st);
+    // plane DFTs of the cells the interior kernel updated
+    if (e == cudaSuccess && use_interior && pl.n) e = launch_plane_dft_box<T>(a, ebox, pl, st);
+    if (prof) cudaEventRecord(ev[3], st);
+    if (e == cudaSuccess) e = launch_shell_E<T>(a, ebox, src, pl, st);
+    if (prof) {
+        cudaEventRecord(ev[4], st);
+        prof_end(ev);
     }
-    return launch_shell_E<T>(a, ebox, src, pl, st);
+    return e;
 }
 
 template cudaError_t launch_step_fused<float>(const YeeArgs<float> &, const SourceList &,

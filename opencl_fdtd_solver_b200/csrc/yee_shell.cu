@@ -21,6 +21,7 @@
 // decoded with 32-bit divisions (consecutive threads take consecutive k).
 #include <cuda_runtime.h>
 
+#include "launch_count.cuh"
 #include "yee_launch.cuh"
 
 namespace fdtd {
@@ -191,6 +192,7 @@ cudaError_t launch_plane_dft_box(const YeeArgs<T> &a, const ShellBox &b, const P
         if (n <= 0) continue;
         k_plane_dft_box<T><<<(unsigned)((n + SHELL_THREADS - 1) / SHELL_THREADS), SHELL_THREADS, 0,
                              st>>>(a, b, pl, q);
+        count_launches(1);
     }
     return cudaGetLastError();
 }
@@ -221,6 +223,7 @@ cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t 
     const unsigned nb = shell_blocks(sp);
     if (nb == 0) return cudaSuccess;
     k_shell_H<T><<<nb, SHELL_THREADS, 0, st>>>(a, sp);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -235,6 +238,7 @@ cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceL
         k_shell_E<T, true><<<nb, SHELL_THREADS, 0, st>>>(a, sp, src, pl);
     else
         k_shell_E<T, false><<<nb, SHELL_THREADS, 0, st>>>(a, sp, src, pl);
+    count_launches(1);
     return cudaGetLastError();
 }
 

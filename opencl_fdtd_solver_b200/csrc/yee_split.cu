@@ -9,6 +9,7 @@
 // reference kernels with every operation rounded separately.
 #include <cuda_runtime.h>
 
+#include "launch_count.cuh"
 #include "yee_cell.cuh"
 #include "yee_launch.cuh"
 
@@ -122,6 +123,7 @@ cudaError_t launch_update_H(const YeeArgs<T> &a, cudaStream_t st) {
     dim3 blk(SPLIT_TK, SPLIT_TJ, 1);
     dim3 grd((a.nz + SPLIT_TK - 1) / SPLIT_TK, (a.ny + SPLIT_TJ - 1) / SPLIT_TJ, a.nx);
     k_update_H<T><<<grd, blk, 0, st>>>(a);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -134,6 +136,7 @@ cudaError_t launch_update_E(const YeeArgs<T> &a, const SourceList &src, const Pl
         k_update_E<T, true><<<grd, blk, 0, st>>>(a, src, pl);
     else
         k_update_E<T, false><<<grd, blk, 0, st>>>(a, src, pl);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -143,6 +146,7 @@ cudaError_t launch_add_source(int nx, int ny, int nz, const fdtd_source &s, T *E
     dim3 blk(128, 1, 1);
     dim3 grd((ny + 127) / 128, nx, 1);
     k_add_source<T><<<grd, blk, 0, st>>>(nx, ny, nz, s, Ex, ce_x);
+    count_launches(1);
     return cudaGetLastError();
 }
 

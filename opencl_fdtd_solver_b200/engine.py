@@ -26,6 +26,7 @@ constructor raises.
 
 from __future__ import annotations
 
+import ctypes
 import logging
 import warnings
 from typing import Sequence
@@ -35,7 +36,6 @@ import numpy as np
 from . import _capi as capi
 from .constants import C0, EPS0, MU0
 from .cpml import build_cpml_profiles, inverse_kappa_dl
-from .materials import yee_edge_ca_cb, yee_edge_ce
 from .plugin import SourceMonitorMixin, register_backend
 
 log = logging.getLogger(__name__)
@@ -277,33 +277,44 @@ class CUDAFDTD(SourceMonitorMixin):
 
     # -------------------------------------------------------------- materials
     def set_epsilon(self, eps_array, sigma_array=None):
-        """Cell-centred εr (and optional σ in S/m) → Yee-edge ``ce`` (and ``ca``) on the device."""
+        """Cell-centred εr (and optional σ in S/m) → Yee-edge ``ce`` (and ``ca``).
+
+        The arrays are uploaded once and the edge average and coefficients are
+        computed on the device in float64 (``fdtd_set_epsilon``), with the same
+        operations as the reference host math (``materials.py:28-88``), so the
+        rounded coefficients are identical to ``yee_edge_ce`` / ``yee_edge_ca_cb``.
+        """
         torch = _torch()
         expected = (self.Nx, self.Ny, self.Nz)
         if tuple(np.shape(eps_array)) != expected:
             raise ValueError(
                 f"Epsilon shape mismatch: expected {expected}, got {tuple(np.shape(eps_array))}")
+        if sigma_array is not None and tuple(np.shape(sigma_array)) != expected:
+            raise ValueError(f"Sigma shape mismatch: expected {expected}, "
+                             f"got {tuple(np.shape(sigma_array))}")
         self._materialize()
         eps = np.asarray(eps_array)
-        if sigma_array is None:
-            coeffs = yee_edge_ce(eps, self.dt, dtype=self.dtype)
-            cas = None
-        else:
-            if tuple(np.shape(sigma_array)) != expected:
-                raise ValueError(f"Sigma shape mismatch: expected {expected}, "
-                                 f"got {tuple(np.shape(sigma_array))}")
-            cas, coeffs = yee_edge_ca_cb(eps, np.asarray(sigma_array), self.dt, dtype=self.dtype)
+        sig = None if sigma_array is None else np.asarray(sigma_array)
+        narrow = eps.dtype == np.float32 and (sig is None or sig.dtype == np.float32)
+        src = np.float32 if narrow else np.float64
         with torch.cuda.stream(self.queue):
-            for a in range(3):
-                self._ce[a].copy_(torch.from_numpy(np.ascontiguousarray(coeffs[a])),
-                                  non_blocking=False)
-            if cas is None:
+            eps_d = torch.from_numpy(np.ascontiguousarray(eps, dtype=src)).to(self.device)
+            sig_d = None
+            if sig is not None:
+                sig_d = torch.from_numpy(np.ascontiguousarray(sig, dtype=src)).to(self.device)
+                if self._ca is None:
+                    self._ca = [torch.empty_like(c) for c in self._ce]
+            ce = (ctypes.c_void_p * 3)(*[c.data_ptr() for c in self._ce])
+            ca = (ctypes.c_void_p * 3)(*([c.data_ptr() for c in self._ca] if sig_d is not None
+                                         else [None, None, None]))
+            capi.run("fdtd_set_epsilon", self._grid, eps_d.data_ptr(),
+                     None if sig_d is None else sig_d.data_ptr(),
+                     capi.FDTD_F32 if narrow else capi.FDTD_F64, float(self.dt), float(EPS0),
+                     ce, ca, self.queue.cuda_stream)
+            if sig_d is None:
                 self._ca = None
-                self.lossy = False
-            else:
-                self._ca = [torch.from_numpy(np.ascontiguousarray(c)).to(self.device)
-                            for c in cas]
-                self.lossy = True
+            self.lossy = sig_d is not None
+            del eps_d, sig_d
         self._refresh_structs()
 
     # ---------------------------------------------------------------- sources

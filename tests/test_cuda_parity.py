@@ -464,3 +464,53 @@ def test_device_status_clean(cuda):
     flags = ctypes.c_int32(-1)
     capi.run("fdtd_device_status", ctypes.byref(flags), 1)
     assert flags.value == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("src_dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("lossy", [False, True])
+def test_device_set_epsilon_equals_host_math(cuda, dtype, src_dtype, lossy):
+    """Coefficients from fdtd_set_epsilon equal the host float64 math bit for bit
+    (reference materials.py:28-88), for float32 and float64 inputs."""
+    from opencl_fdtd_solver_b200 import materials
+
+    rng = np.random.default_rng(11)
+    shape = (13, 17, 24)
+    eps = (1 + 11 * rng.random(shape)).astype(src_dtype)
+    sig = (0.5 * rng.random(shape)).astype(src_dtype) if lossy else None
+    g = cuda.CUDAFDTD(shape, 1e-3, npml=3, dtype=dtype)
+    g.set_epsilon(eps, sigma_array=sig)
+    co = g.coefficient_tensors()
+    g.synchronize()
+    if lossy:
+        ca, cb = materials.yee_edge_ca_cb(eps, sig, g.dt, dtype)
+        for a in range(3):
+            assert np.array_equal(co["ca"][a].cpu().numpy(), ca[a])
+            assert np.array_equal(co["ce"][a].cpu().numpy(), cb[a])
+    else:
+        ce = materials.yee_edge_ce(eps, g.dt, dtype)
+        assert co["ca"] is None
+        for a in range(3):
+            assert np.array_equal(co["ce"][a].cpu().numpy(), ce[a])
+
+
+def test_launch_counter_and_step_profile(cuda):
+    import ctypes
+
+    from opencl_fdtd_solver_b200 import _capi as capi
+
+    g = cuda.CUDAFDTD((40, 36, 48), 1e-3, npml=6)
+    cuda.CUDAPlaneDFTMonitor(g, 2, 20, [30e9])
+    g.run(2)
+    g.synchronize()
+    n0 = capi.lib().fdtd_launch_count()
+    capi.run("fdtd_profile_steps", 1)
+    g.run(5)
+    capi.run("fdtd_profile_steps", 0)
+    ms = (ctypes.c_double * 4)()
+    n = ctypes.c_int32()
+    capi.run("fdtd_profile_read", ms, ctypes.byref(n))
+    assert n.value == 5
+    assert all(v > 0 for v in ms)
+    # shell H, interior, plane DFT of the interior, shell E per step
+    assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
