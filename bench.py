@@ -15,7 +15,11 @@ independent replica of the workload (the path is one grid per GPU here), timing
 is the max over ranks, and ``value`` is the total cell updates of all ranks per
 second ("scaling": "weak").
 
-The same line carries ``adjoint``: the ε-gradient leg at 160×160×96 FP32 (npml 12,
+The line also carries ``n2f``: the near-to-far contraction of a 320³ box
+(614,400 face samples x 4 currents x 32 frequencies, complex64) onto 361 x 181
+directions in split-BF16 and TF32 on the tensor cores, timed by CUDA events, with
+its error against the float64 direct sum on every 64th direction.
+It also carries ``adjoint``: the ε-gradient leg at 160×160×96 FP32 (npml 12,
 96×96×16 design box, Jx sheet at 30 GHz, 3000 steps, checkpoints every 100 steps,
 objective Σ|Ex(30 GHz)|² over a 32×32 patch): ``t_grad / t_forward`` by CUDA events,
 and the gradient against central differences (h = 1e-3) at 16 seeded voxels in FP64.
@@ -416,6 +420,9 @@ def run_b200_arm(args, rank, world, local):
     }
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if not args.no_n2f:
+        barrier(world)
+        line["n2f"] = run_n2f_leg(args)
     return line
 
 
@@ -551,6 +558,93 @@ def run_adjoint_leg(args):
     }
 
 
+# ------------------------------------------------------------------- n2f leg
+def measured_tensor():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+        except Exception:
+            pass
+    return 1590.0, "fallback"
+
+
+def n2f_faces(n, nfreq, dl=1e-3, seed=4321, rho0=100.0):
+    """Six faces of an n³ box: seeded complex Gaussian currents (complex64) under
+    exp(-(ρ/ρ0)²), ρ the distance from the face centre in cells."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import N2FFace
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    ra = torch.arange(n, device="cuda", dtype=torch.float32) - (n - 1) / 2
+    env = torch.exp(-(ra[:, None] ** 2 + ra[None, :] ** 2) / rho0**2)
+    faces = []
+    for normal in range(3):
+        for side in (0, 1):
+            re = torch.randn((nfreq, n, n, 4), generator=g, device="cuda")
+            im = torch.randn((nfreq, n, n, 4), generator=g, device="cuda")
+            cur = torch.complex(re, im) * env[None, :, :, None]
+            faces.append(N2FFace(normal=normal, x_n=(side - 0.5) * n * dl,
+                                 o_p=(-n / 2 + 0.5) * dl, o_q=(-n / 2 + 0.5) * dl, pitch=dl,
+                                 cur=cur.contiguous()))
+    return faces
+
+
+def n2f_directions(ntheta=361, nphi=181):
+    th = np.linspace(0.0, np.pi, ntheta)
+    ph = np.linspace(0.0, np.pi, nphi)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    return np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1).reshape(-1, 3)
+
+
+def run_n2f_leg(args):
+    """The near-to-far contraction: 6 faces of an n³ box x 4 currents x nfreq
+    frequencies onto 361 x 181 directions, split-BF16 and TF32 on the tensor cores,
+    checked against the float64 direct sum on every 64th direction."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import near2far_contract
+
+    n, nfreq = args.n2f_size, args.n2f_freqs
+    faces = n2f_faces(n, nfreq)
+    dirs = n2f_directions()
+    freqs = np.linspace(10e9, 40e9, nfreq)
+    n_obs, ns = dirs.shape[0], 6 * n * n
+    flops = 8.0 * n_obs * ns * 4 * nfreq
+    peak, peak_kind = measured_tensor()
+    st = torch.cuda.current_stream()
+    out, modes = {}, {}
+    for mode in ("bf16x3", "tf32"):
+        near2far_contract(faces, freqs, dirs, mode=mode)
+        best, res = None, None
+        for _ in range(3):
+            ms, r = timed(lambda: near2far_contract(faces, freqs, dirs, mode=mode), st)
+            if best is None or ms < best:
+                best, res = ms, r
+        out[mode] = res
+        modes[mode] = {"ms": round(best, 2), "alg_tflops": round(flops / best / 1e9, 1),
+                       "frac_of_bf16_peak": round(flops / best / 1e9 / peak, 4),
+                       "mma_products": 3 if mode == "bf16x3" else 1}
+    sub = np.arange(0, n_obs, 64)
+    t64, ref = timed(lambda: near2far_contract(faces, freqs, dirs[sub], mode="fp64"), st)
+    ref = ref.cpu().numpy()
+    for mode, res in out.items():
+        o = res.cpu().numpy()[:, sub].astype(np.complex128)
+        modes[mode]["rel_err_vs_fp64"] = float(np.linalg.norm(o - ref) / np.linalg.norm(ref))
+        modes[mode]["max_err_over_peak"] = float(np.abs(o - ref).max() / np.abs(ref).max())
+    t64_full = t64 * n_obs / sub.size
+    return {
+        "workload": f"n2f_box{n}^3_6faces_{ns}samples_x4_{nfreq}freqs_to_361x181_dirs",
+        "alg_flops": flops, "peak_tflops": peak, "peak_source": peak_kind,
+        "modes": modes,
+        "fp64_direct_ms_subset": round(t64, 1), "fp64_subset_dirs": int(sub.size),
+        "fp64_direct_ms_extrapolated": round(t64_full, 1),
+        "speedup_bf16x3_vs_fp64_direct": round(t64_full / modes["bf16x3"]["ms"], 1),
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -565,6 +659,11 @@ def main(argv=None):
                     help="CPU-baseline sample length beside the GPU arm")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint-gradient leg (t_grad / t_forward, FD check)")
+    ap.add_argument("--no-n2f", action="store_true", help="skip the near-to-far contraction leg")
+    ap.add_argument("--only", choices=("n2f", "adjoint"),
+                    help="run one auxiliary leg alone and print its object (profiling)")
+    ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
+    ap.add_argument("--n2f-freqs", type=int, default=32)
     ap.add_argument("--cpu-budget", type=float, default=150.0,
                     help="time budget of the --impl reference arm's timed steps")
     args = ap.parse_args(argv)
@@ -578,6 +677,11 @@ def main(argv=None):
             print(json.dumps(line), flush=True)
         return 0
     rank, world, local = dist_setup(args.gpus)
+    if args.only:
+        res = run_n2f_leg(args) if args.only == "n2f" else run_adjoint_leg(args)
+        if rank == 0:
+            print(json.dumps({args.only: res}), flush=True)
+        return 0
     line = run_b200_arm(args, rank, world, local)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -184,6 +184,46 @@ int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl,
                   double k_wave, double eta0, const double *obs_xyz, int32_t n_obs,
                   double *nl_scratch, double *eh, void *stream);
 
+/* ---- near-to-far contraction on the tensor cores ------------------------ */
+/* NL[f][o][6] = (Nx, Ny, Nz, Lx, Ly, Lz)(r̂_o, f) = Σ_faces Σ_{p,q}
+ * e^{+j 2π f r̂_o·r'_{pq}/c0} cur[f][p][q][c], the surface sums that
+ * farfield_accumulate_nl (dft_farfield.cl:372-556) forms for one direction at a
+ * time, for many directions and frequencies at once.  r'_{pq} is
+ * x_n along the face normal and (o_p + p·pitch, o_q + q·pitch) along its two
+ * in-face axes (in x, y, z order); cur holds the face's four tangential
+ * currents J_p, J_q, M_p, M_q (J = n̂×H, M = −n̂×E) with the quadrature
+ * weights already applied.  The far field then follows as in
+ * dft_farfield.cl:559-635. */
+#define FDTD_N2F_BF16X3 0  /* tcgen05 kind::f16, split BF16 (hi·hi + hi·lo + lo·hi), FP32 accumulate */
+#define FDTD_N2F_TF32 1    /* tcgen05 kind::tf32, FP32 accumulate                          */
+#define FDTD_N2F_FP64 2    /* float64 direct sum on the CUDA cores (the reference transform) */
+
+typedef struct {
+    int32_t normal;        /* axis normal to the face: 0, 1, 2                     */
+    int32_t np, nq;        /* samples along the two in-face axes                    */
+    int32_t pad_;
+    double x_n;            /* face coordinate along its normal (m)                  */
+    double o_p, o_q;       /* in-face coordinates of sample (0, 0) (m)              */
+    double pitch;          /* sample spacing (m)                                    */
+    const void *cur;       /* device, complex [nfreq][np][nq][4] of cur_dtype       */
+} fdtd_n2f_face;
+
+/* Workspace bytes fdtd_n2f_contract needs for these faces (0 for FP64). */
+int fdtd_n2f_workspace(const fdtd_n2f_face *faces, int32_t nfaces, int32_t nfreq, int32_t n_obs,
+                       int32_t mode, uint64_t *bytes);
+
+/* faces: host array of nfaces (1..6) face descriptors; cur_dtype: FDTD_F32
+ * (complex64) or FDTD_F64 (complex128); freqs: device, nfreq doubles (Hz);
+ * dirs: device, n_obs unit vectors (float64 xyz); nl: device, complex64
+ * [nfreq][n_obs][6] for the tensor-core modes, complex128 for FDTD_N2F_FP64.
+ * The tensor-core modes pack the currents into the workspace (256-byte
+ * aligned), run one CTA per (128 directions, face, frequency) and reduce the
+ * faces; bounded waits set bit 1 of fdtd_device_status on timeout. */
+int fdtd_n2f_contract(const fdtd_n2f_face *faces, int32_t nfaces, int32_t cur_dtype,
+                      const double *freqs, int32_t nfreq, const double *dirs, int32_t n_obs,
+                      int32_t mode, void *workspace, uint64_t workspace_bytes, void *nl,
+                      void *stream);
+
 /* ---- adjoint (ε-gradient) ------------------------------------------------ */
 /* No reference counterpart: the reference has no gradient.  These entry points
  * run the reverse-time sweep of the transposed (discrete adjoint) Yee/CPML
@@ -282,7 +322,8 @@ int64_t fdtd_launch_count(void);
 const char *fdtd_last_error(void);
 
 /* Device-side error flags raised by kernels since the last reset (bit 0: a
- * bounded wait in the fused step timed out).  Synchronises with the device to
+ * bounded wait in the fused step timed out; bit 1: one in the near-to-far
+ * contraction did).  Synchronises with the device to
  * read the flag; clears it when reset != 0.  No reference counterpart (the
  * reference kernels have no device-side waits). */
 int fdtd_device_status(int32_t *flags, int32_t reset);

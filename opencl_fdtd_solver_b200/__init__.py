@@ -8,6 +8,8 @@ with ``CUDAFDTD`` / ``CUDANear2FarMonitor`` in place of the OpenCL classes):
 * ``CUDANear2FarMonitor`` — Huygens-box DFT + far field
 * ``CUDAPlaneDFTMonitor`` — single-plane DFT fused into the E update
 * ``StepCallback``, ``SourceMonitorMixin``, ``BACKENDS``, ``get_backend``
+* ``near2far_contract``, ``N2FFace``, ``box_faces`` — near-to-far sums for many
+  directions and frequencies on the tensor cores (split-BF16 / TF32) or in FP64
 * ``DFTObjective``, ``EpsilonAdjoint``, ``EpsilonObjective`` — discrete-adjoint
   ε-gradient of a plane-DFT objective (``EpsilonObjective`` is the
   ``torch.autograd.Function``)
@@ -21,6 +23,7 @@ from .adjoint import DFTObjective, EpsilonAdjoint, EpsilonObjective, epsilon_obj
 from .constants import C0, EPS0, ETA0, MU0
 from .engine import CUDAFDTD
 from .monitors import CUDANear2FarMonitor, CUDAPlaneDFTMonitor
+from .n2f import N2FFace, box_faces, near2far_contract
 from .plugin import BACKENDS, SourceMonitorMixin, StepCallback, get_backend, register_backend
 
 __all__ = [
@@ -36,6 +39,9 @@ __all__ = [
     "BACKENDS",
     "get_backend",
     "register_backend",
+    "near2far_contract",
+    "N2FFace",
+    "box_faces",
     "DFTObjective",
     "EpsilonAdjoint",
     "EpsilonObjective",

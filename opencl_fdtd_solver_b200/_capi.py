@@ -10,7 +10,7 @@ engine fails loudly.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_void_p
+from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_uint64, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libfdtd_b200.so"
@@ -28,6 +28,9 @@ FDTD_MAX_FREQS = 64
 FDTD_NOALLOC_MAX_FACE = 1024 * 256
 FDTD_SRC_JX = 0
 FDTD_SRC_EX = 1
+FDTD_N2F_BF16X3 = 0
+FDTD_N2F_TF32 = 1
+FDTD_N2F_FP64 = 2
 
 V3 = c_void_p * 3
 V6 = c_void_p * 6
@@ -81,6 +84,12 @@ class GradBox(Structure):
                 ("e_prev", c_void_p), ("g", c_void_p)]
 
 
+class N2FFace(Structure):
+    _fields_ = [("normal", c_int32), ("np", c_int32), ("nq", c_int32), ("pad_", c_int32),
+                ("x_n", c_double), ("o_p", c_double), ("o_q", c_double), ("pitch", c_double),
+                ("cur", c_void_p)]
+
+
 # name -> (restype, argtypes); every symbol include/fdtd_b200.h declares.
 SIGNATURES = {
     "fdtd_update_H": (c_int32, [POINTER(Grid), POINTER(Fields), POINTER(Cpml), c_void_p]),
@@ -109,6 +118,11 @@ SIGNATURES = {
     "fdtd_profile_steps": (c_int32, [c_int32]),
     "fdtd_profile_read": (c_int32, [POINTER(c_double), POINTER(c_int32)]),
     "fdtd_launch_count": (c_int64, []),
+    "fdtd_n2f_workspace": (c_int32, [POINTER(N2FFace), c_int32, c_int32, c_int32, c_int32,
+                                     POINTER(c_uint64)]),
+    "fdtd_n2f_contract": (c_int32, [POINTER(N2FFace), c_int32, c_int32, c_void_p, c_int32,
+                                    c_void_p, c_int32, c_int32, c_void_p, c_uint64, c_void_p,
+                                    c_void_p]),
     "fdtd_last_error": (c_char_p, []),
     "fdtd_device_status": (c_int32, [POINTER(c_int32), c_int32]),
     "fdtd_version": (c_char_p, []),

@@ -11,6 +11,7 @@
 #include "../../include/fdtd_b200.h"
 #include "yee_launch.cuh"
 #include "adjoint.cuh"
+#include "n2f.cuh"
 
 namespace fdtd {
 template <typename T>
@@ -308,6 +309,60 @@ fdtd::AdjGrad<T> make_grad(const fdtd_grad_box *gb) {
     return r;
 }
 
+// ---- near-to-far contraction ------------------------------------------------
+struct N2FPlan {
+    fdtd::n2f::Params P;
+    uint64_t btile_bytes, partial_off, total;
+};
+
+int plan_n2f(const fdtd_n2f_face *faces, int nfaces, int nfreq, int n_obs, int mode, N2FPlan &pl) {
+    if (!faces) return fail(FDTD_ERR_INVALID, "faces is NULL");
+    if (nfaces < 1 || nfaces > 6) return fail(FDTD_ERR_INVALID, "nfaces %d outside [1, 6]", nfaces);
+    if (nfreq < 1 || nfreq > 65535) return fail(FDTD_ERR_INVALID, "nfreq %d outside [1, 65535]", nfreq);
+    if (n_obs < 1) return fail(FDTD_ERR_INVALID, "n_obs must be positive, got %d", n_obs);
+    if (mode != FDTD_N2F_BF16X3 && mode != FDTD_N2F_TF32 && mode != FDTD_N2F_FP64)
+        return fail(FDTD_ERR_INVALID, "unknown near-to-far mode %d", mode);
+    memset(&pl, 0, sizeof(pl));
+    auto &P = pl.P;
+    P.n_obs = n_obs;
+    P.nfaces = nfaces;
+    const bool tc = mode != FDTD_N2F_FP64;
+    const int kr = tc ? fdtd::n2f::k_real_per_step(mode) : 16;
+    const int64_t bcopy = tc ? fdtd::n2f::b_copy_bytes(mode) : 0;
+    uint64_t off = 0;
+    for (int f = 0; f < nfaces; ++f) {
+        const fdtd_n2f_face &F = faces[f];
+        if (F.normal < 0 || F.normal > 2)
+            return fail(FDTD_ERR_INVALID, "face %d: normal axis %d", f, F.normal);
+        if (F.np < 1 || F.nq < 1 || F.np > (1 << 20) || F.nq > (1 << 20))
+            return fail(FDTD_ERR_INVALID, "face %d: sample counts %d x %d", f, F.np, F.nq);
+        if (!F.cur) return fail(FDTD_ERR_INVALID, "face %d: cur is NULL", f);
+        if (!(F.pitch > 0)) return fail(FDTD_ERR_INVALID, "face %d: pitch must be positive", f);
+        auto &G = P.face[f];
+        G.axis_n = F.normal;
+        G.axis_p = F.normal == 0 ? 1 : 0;
+        G.axis_q = F.normal == 2 ? 1 : 2;
+        G.np = F.np;
+        G.nq = F.nq;
+        G.ks = (2 * F.np + kr - 1) / kr;
+        G.nt = (F.nq + fdtd::n2f::QT - 1) / fdtd::n2f::QT;
+        G.x_n = F.x_n;
+        G.o_p = F.o_p;
+        G.o_q = F.o_q;
+        G.pitch = F.pitch;
+        G.b_freq_stride = (int64_t)G.ks * G.nt * bcopy;
+        G.b_off = (int64_t)off;
+        off += (uint64_t)G.b_freq_stride * nfreq;
+        P.cur[f] = F.cur;
+        const int map[4] = {G.axis_p, G.axis_q, 3 + G.axis_p, 3 + G.axis_q};
+        for (int c = 0; c < 4; ++c) P.comp_map[f * 4 + c] = map[c];
+    }
+    pl.btile_bytes = off;
+    pl.partial_off = (off + 255) & ~(uint64_t)255;
+    pl.total = tc ? pl.partial_off + (uint64_t)nfreq * nfaces * n_obs * 4 * 8 : 0;
+    return FDTD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -320,7 +375,7 @@ int fdtd_device_status(int32_t *flags, int32_t reset) {
     if (!flags) return fail(FDTD_ERR_INVALID, "flags is NULL");
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_status(e, "device_status");
-    *flags = fdtd::read_fused_error(reset);
+    *flags = fdtd::read_fused_error(reset) | (fdtd::n2f::read_error(reset) ? 2 : 0);
     return cuda_status(cudaGetLastError(), "device_status");
 }
 
@@ -571,6 +626,58 @@ int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int
                                                          (double *const *)cav, st);
     }
     return cuda_status(e, "set_epsilon");
+}
+
+int fdtd_n2f_workspace(const fdtd_n2f_face *faces, int32_t nfaces, int32_t nfreq, int32_t n_obs,
+                       int32_t mode, uint64_t *bytes) {
+    if (!bytes) return fail(FDTD_ERR_INVALID, "bytes is NULL");
+    N2FPlan pl;
+    int rc;
+    if ((rc = plan_n2f(faces, nfaces, nfreq, n_obs, mode, pl))) return rc;
+    *bytes = pl.total;
+    return FDTD_OK;
+}
+
+int fdtd_n2f_contract(const fdtd_n2f_face *faces, int32_t nfaces, int32_t cur_dtype,
+                      const double *freqs, int32_t nfreq, const double *dirs, int32_t n_obs,
+                      int32_t mode, void *workspace, uint64_t workspace_bytes, void *nl,
+                      void *stream) {
+    N2FPlan pl;
+    int rc;
+    if ((rc = plan_n2f(faces, nfaces, nfreq, n_obs, mode, pl))) return rc;
+    if (cur_dtype != FDTD_F32 && cur_dtype != FDTD_F64)
+        return fail(FDTD_ERR_INVALID, "cur_dtype must be FDTD_F32 or FDTD_F64, got %d", cur_dtype);
+    if (!freqs || !dirs || !nl) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    auto &P = pl.P;
+    P.dirs = dirs;
+    P.freqs = freqs;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if (mode == FDTD_N2F_FP64) {
+        e = cur_dtype == FDTD_F32 ? fdtd::n2f::launch_fp64<float2>(P, nfreq, (double2 *)nl, st)
+                                  : fdtd::n2f::launch_fp64<double2>(P, nfreq, (double2 *)nl, st);
+        return cuda_status(e, "n2f_contract");
+    }
+    if (!workspace || workspace_bytes < pl.total)
+        return fail(FDTD_ERR_INVALID, "workspace of %llu bytes is smaller than the %llu needed",
+                    (unsigned long long)workspace_bytes, (unsigned long long)pl.total);
+    if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+        return fail(FDTD_ERR_INVALID, "workspace must be 256-byte aligned");
+    unsigned char *ws = (unsigned char *)workspace;
+    for (int f = 0; f < nfaces; ++f) {
+        const auto &G = P.face[f];
+        e = cur_dtype == FDTD_F32
+                ? fdtd::n2f::launch_pack<float2>(mode, (const float2 *)P.cur[f], nfreq, G.np, G.nq,
+                                                 G.ks, G.nt, ws + G.b_off, st)
+                : fdtd::n2f::launch_pack<double2>(mode, (const double2 *)P.cur[f], nfreq, G.np,
+                                                  G.nq, G.ks, G.nt, ws + G.b_off, st);
+        if (e != cudaSuccess) return cuda_status(e, "n2f_pack");
+    }
+    P.btiles = ws;
+    P.partial = (float2 *)(ws + pl.partial_off);
+    if ((e = fdtd::n2f::launch_contract(mode, P, nfreq, st)) != cudaSuccess)
+        return cuda_status(e, "n2f_contract");
+    return cuda_status(fdtd::n2f::launch_combine(P, nfreq, (float2 *)nl, st), "n2f_combine");
 }
 
 }  // extern "C"

@@ -44,7 +44,7 @@ def test_ctypes_structs_match_c_header(tmp_path):
     structs = {"fdtd_grid": capi.Grid, "fdtd_fields": capi.Fields, "fdtd_cpml": capi.Cpml,
                "fdtd_source": capi.Source, "fdtd_plane_dft": capi.PlaneDft, "fdtd_box": capi.Box,
                "fdtd_adjoint_fields": capi.AdjointFields, "fdtd_adjoint_seed": capi.AdjointSeed,
-               "fdtd_grad_box": capi.GradBox}
+               "fdtd_grad_box": capi.GradBox, "fdtd_n2f_face": capi.N2FFace}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fdtd_b200.h"',
              'int main(void) {']
     for cname, py in structs.items():
