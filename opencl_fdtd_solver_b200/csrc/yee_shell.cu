@@ -110,16 +110,18 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     a.H_next[2][idx] = hz;
 }
 
-__device__ __noinline__ void shell_dft(const PlaneList &planes, int i, int j, int k, int nx,
+// planes points at the kernel's __grid_constant__ parameter, so the call takes
+// no local copy of the descriptor list.
+__device__ __noinline__ void shell_dft(const PlaneList *planes, int i, int j, int k, int nx,
                                        int ny, int nz, double ex, double ey, double ez,
                                        double hx, double hy, double hz) {
     const double v[6] = {ex, ey, ez, hx, hy, hz};
-    plane_dft_cell(planes, i, j, k, nx, ny, nz, v);
+    plane_dft_cell(*planes, i, j, k, nx, ny, nz, v);
 }
 
 template <typename T, bool LOSSY>
 __global__ void __launch_bounds__(SHELL_THREADS)
-    k_shell_E(YeeArgs<T> a, ShellPlan sp, SourceList src, PlaneList planes) {
+    k_shell_E(YeeArgs<T> a, ShellPlan sp, SourceList src, const __grid_constant__ PlaneList planes) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, npml = a.npml;
     int i, j, k;
     if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, nx, ny, nz, sp, i, j, k)) return;
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     a.E_next[1][idx] = ey;
     a.E_next[2][idx] = ez;
     if (planes.n && plane_any_hit(planes, i, j, k))
-        shell_dft(planes, i, j, k, nx, ny, nz, (double)ex, (double)ey, (double)ez, (double)hx0,
+        shell_dft(&planes, i, j, k, nx, ny, nz, (double)ex, (double)ey, (double)ez, (double)hx0,
                   (double)hy0, (double)hz0);
 }
 
