@@ -622,7 +622,7 @@ namespace {
 struct StepProfiler {
     std::mutex mu;
     bool on = false;
-    std::vector<std::array<cudaEvent_t, 5>> pending;
+    std::vector<std::array<cudaEvent_t, 6>> pending;
     double ms[4] = {0.0, 0.0, 0.0, 0.0};
     int steps = 0;
 };
@@ -632,10 +632,13 @@ StepProfiler g_prof;
 cudaError_t prof_flush_locked() {
     cudaError_t err = cudaSuccess;
     for (auto &ev : g_prof.pending) {
-        cudaError_t e = cudaEventSynchronize(ev[4]);
+        // ev: 0 start, 1 shell H done (side stream), 2 interior done, 3 joined,
+        // 4 plane DFT done, 5 shell E done
+        cudaError_t e = cudaEventSynchronize(ev[5]);
+        const int from[4] = {0, 0, 3, 4}, to[4] = {1, 2, 4, 5};
         for (int s = 0; s < 4 && e == cudaSuccess; ++s) {
             float t = 0.f;
-            e = cudaEventElapsedTime(&t, ev[s], ev[s + 1]);
+            e = cudaEventElapsedTime(&t, ev[from[s]], ev[to[s]]);
             g_prof.ms[s] += t;
         }
         if (e != cudaSuccess) err = e;
@@ -646,10 +649,10 @@ cudaError_t prof_flush_locked() {
     return err;
 }
 
-bool prof_begin(std::array<cudaEvent_t, 5> &ev) {
+bool prof_begin(std::array<cudaEvent_t, 6> &ev) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     if (!g_prof.on) return false;
-    for (int s = 0; s < 5; ++s)
+    for (int s = 0; s < 6; ++s)
         if (cudaEventCreate(&ev[s]) != cudaSuccess) {
             for (int q = 0; q < s; ++q) cudaEventDestroy(ev[q]);
             return false;
@@ -657,10 +660,37 @@ bool prof_begin(std::array<cudaEvent_t, 5> &ev) {
     return true;
 }
 
-void prof_end(const std::array<cudaEvent_t, 5> &ev) {
+void prof_end(const std::array<cudaEvent_t, 6> &ev) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     g_prof.pending.push_back(ev);
     if (g_prof.pending.size() >= 2048) prof_flush_locked();
+}
+// Side stream (per host thread and device) on which the CPML-shell H kernel
+// runs concurrently with the interior kernel: the two are independent (the
+// interior kernel recomputes every H it needs from E and H), so the latency-
+// bound shell fills the bandwidth the interior kernel leaves.  Joined back to
+// the caller's stream by an event before the E half.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+thread_local std::unordered_map<int, SideStream> t_side;
+
+cudaError_t side_stream(SideStream **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    auto it = t_side.find(dev);
+    if (it == t_side.end()) {
+        SideStream ss;
+        if ((e = cudaStreamCreateWithFlags(&ss.s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+        it = t_side.emplace(dev, ss).first;
+    }
+    *out = &it->second;
+    return cudaSuccess;
 }
 }  // namespace
 
@@ -706,19 +736,41 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
         ebox.lo[d] = use_interior ? a.npml + 1 : 0;
         ebox.hi[d] = use_interior ? n[d] - a.npml : 0;
     }
-    std::array<cudaEvent_t, 5> ev;
+    SideStream *side = nullptr;
+    if (use_interior) {
+        cudaError_t e = side_stream(&side);
+        if (e != cudaSuccess) return e;
+    }
+    std::array<cudaEvent_t, 6> ev;
     const bool prof = prof_begin(ev);
     if (prof) cudaEventRecord(ev[0], st);
-    cudaError_t e = launch_shell_H<T>(a, hbox, st);
-    if (prof) cudaEventRecord(ev[1], st);
-    if (e == cudaSuccess && use_interior) e = launch_interior<T>(a, maps, hbox, src, st);
-    if (prof) cudaEventRecord(ev[2], st);
+    cudaError_t e = cudaSuccess;
+    if (use_interior) {
+        // shell H on the side stream, concurrent with the interior kernel
+        if ((e = cudaEventRecord(side->fork, st)) == cudaSuccess &&
+            (e = cudaStreamWaitEvent(side->s, side->fork, 0)) == cudaSuccess)
+            e = launch_shell_H<T>(a, hbox, side->s);
+        if (prof) cudaEventRecord(ev[1], side->s);
+        cudaError_t e2 = cudaEventRecord(side->join, side->s);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = launch_interior<T>(a, maps, hbox, src, st);
+        if (prof) cudaEventRecord(ev[2], st);
+        e2 = cudaStreamWaitEvent(st, side->join, 0);
+        if (e == cudaSuccess) e = e2;
+    } else {
+        e = launch_shell_H<T>(a, hbox, st);
+        if (prof) {
+            cudaEventRecord(ev[1], st);
+            cudaEventRecord(ev[2], st);
+        }
+    }
+    if (prof) cudaEventRecord(ev[3], st);
     // plane DFTs of the cells the interior kernel updated
     if (e == cudaSuccess && use_interior && pl.n) e = launch_plane_dft_box<T>(a, ebox, pl, st);
-    if (prof) cudaEventRecord(ev[3], st);
+    if (prof) cudaEventRecord(ev[4], st);
     if (e == cudaSuccess) e = launch_shell_E<T>(a, ebox, src, pl, st);
     if (prof) {
-        cudaEventRecord(ev[4], st);
+        cudaEventRecord(ev[5], st);
         prof_end(ev);
     }
     return e;
