@@ -401,12 +401,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             if (MODE == FDTD_N2F_BF16X3) {
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
-                    __align__(16) __nv_bfloat16 hi[8], lo[8];
+                    // packed conversions: two values per cvt.rn.bf16x2.f32
+                    __align__(16) __nv_bfloat162 hi[4], lo[4];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const float x = vals[8 * c + e];
-                        hi[e] = __float2bfloat16_rn(x);
-                        lo[e] = __float2bfloat16_rn(x - __bfloat162float(hi[e]));
+                    for (int e = 0; e < 4; ++e) {
+                        const float x0 = vals[8 * c + 2 * e], x1 = vals[8 * c + 2 * e + 1];
+                        hi[e] = __floats2bfloat162_rn(x0, x1);
+                        const float2 hf = __bfloat1622float2(hi[e]);
+                        lo[e] = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
                     }
                     const int off = c * (BM / 8) * 128 + roff;
                     *reinterpret_cast<uint4 *>(st + off) = *reinterpret_cast<const uint4 *>(hi);
