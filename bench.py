@@ -457,7 +457,7 @@ def design_eps(seed=2024, corr=6.0):
     return 1.0 + 3.0 / (1.0 + np.exp(-g))
 
 
-def adjoint_problem(dtype):
+def adjoint_problem(dtype, n_steps=ADJ_STEPS):
     from opencl_fdtd_solver_b200 import CUDAFDTD, DFTObjective, EpsilonAdjoint
 
     fd = CUDAFDTD(ADJ_SHAPE, 1e-3, npml=ADJ_NPML, dtype=dtype)
@@ -465,7 +465,7 @@ def adjoint_problem(dtype):
     fd.add_source(lambda f: f.add_source_Jx(s["z"], gaussian_sine(f.t), s["i0"], s["i1"],
                                             s["j0"], s["j1"], rim_taper=True))
     obj = DFTObjective("z", ADJ_PLANE, ADJ_PATCH, [ADJ_FREQ], ("Ex",))
-    return EpsilonAdjoint(fd, ADJ_DESIGN, ADJ_STEPS, obj, checkpoint_every=ADJ_K)
+    return EpsilonAdjoint(fd, ADJ_DESIGN, n_steps, obj, checkpoint_every=ADJ_K)
 
 
 def plain_forward(adj, eps_d):
@@ -508,7 +508,7 @@ def run_adjoint_leg(args):
     import torch
 
     eps_d = design_eps()
-    adj = adjoint_problem(np.float32)
+    adj = adjoint_problem(np.float32, args.adj_steps)
     st = adj.fdtd.queue
     adj.value_and_grad(eps_d)  # warm-up
     plain_forward(adj, eps_d)
@@ -517,11 +517,11 @@ def run_adjoint_leg(args):
                              key=lambda r: r[0])
     del adj
     torch.cuda.empty_cache()
-    adj64 = adjoint_problem(np.float64)
+    adj64 = adjoint_problem(np.float64, args.adj_steps)
     t64, (J64, g64) = timed(lambda: adj64.value_and_grad(eps_d), adj64.fdtd.queue)
     rng = np.random.default_rng(16)
     dims = g64.shape
-    voxels = [tuple(int(rng.integers(0, d)) for d in dims) for _ in range(16)]
+    voxels = [tuple(int(rng.integers(0, d)) for d in dims) for _ in range(args.adj_fd_voxels)]
     h = 1e-3
     fd_g = []
     for v in voxels:
@@ -539,7 +539,7 @@ def run_adjoint_leg(args):
     torch.cuda.empty_cache()
     return {
         "workload": (f"adjoint_{ADJ_SHAPE[0]}x{ADJ_SHAPE[1]}x{ADJ_SHAPE[2]}_npml{ADJ_NPML}_"
-                     f"design{dims[0]}x{dims[1]}x{dims[2]}_jx_sheet_30GHz_{ADJ_STEPS}steps_"
+                     f"design{dims[0]}x{dims[1]}x{dims[2]}_jx_sheet_30GHz_{args.adj_steps}steps_"
                      f"patch32x32_K{ADJ_K}"),
         "t_forward_ms": round(t_fwd, 2),
         "t_grad_ms": round(t_grad, 2),
@@ -548,10 +548,11 @@ def run_adjoint_leg(args):
         "fd_gradient_cost_forward_solves": n_design + 1,
         "fd_gradient_ms_extrapolated": round((n_design + 1) * t_fwd, 1),
         "speedup_vs_fd_gradient": round((n_design + 1) * t_fwd / t_grad, 1),
-        "fd_check": {"voxels": len(voxels), "h": h, "dtype": "f64",
-                     "rel_err": float(np.linalg.norm(ad64 - fd_g) / np.linalg.norm(fd_g)),
-                     "rel_err_fp32_adjoint_vs_fd": float(np.linalg.norm(ad32 - fd_g)
-                                                         / np.linalg.norm(fd_g))},
+        "fd_check": ({"voxels": len(voxels), "h": h, "dtype": "f64",
+                      "rel_err": float(np.linalg.norm(ad64 - fd_g) / np.linalg.norm(fd_g)),
+                      "rel_err_fp32_adjoint_vs_fd": float(np.linalg.norm(ad32 - fd_g)
+                                                          / np.linalg.norm(fd_g))}
+                     if voxels else None),
         "fp32_vs_fp64_grad_rel_err": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
         "J_fp32": J32, "J_fp64": J64, "t_grad_fp64_ms": round(t64, 2),
         "design_eps": "1 + 3 sigmoid(GRF), sigma 6 cells, seed 2024",
@@ -664,6 +665,9 @@ def main(argv=None):
                     help="run one auxiliary leg alone and print its object (profiling)")
     ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
     ap.add_argument("--n2f-freqs", type=int, default=32)
+    ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS, help="time steps per adjoint solve")
+    ap.add_argument("--adj-fd-voxels", type=int, default=16,
+                    help="design voxels checked by central differences")
     ap.add_argument("--cpu-budget", type=float, default=150.0,
                     help="time budget of the --impl reference arm's timed steps")
     args = ap.parse_args(argv)

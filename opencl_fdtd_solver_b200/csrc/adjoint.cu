@@ -121,6 +121,25 @@ __device__ __forceinline__ void add_seed(const AdjSeed &sd, int i, int j, int k,
     }
 }
 
+// G_c += Ē_c·(E_c^{n+1} − E_c^n) for a cell of the gradient box.
+template <typename T>
+__device__ __forceinline__ void adj_grad_cell(const AdjGrad<T> &gb, int i, int j, int k, T ex,
+                                              T ey, T ez) {
+    if (i < gb.lo[0] || i >= gb.hi[0] || j < gb.lo[1] || j >= gb.hi[1] || k < gb.lo[2] ||
+        k >= gb.hi[2])
+        return;
+    const int by = gb.hi[1] - gb.lo[1], bz = gb.hi[2] - gb.lo[2];
+    const int64_t nb = (int64_t)(gb.hi[0] - gb.lo[0]) * by * bz;
+    const int64_t loc = ((int64_t)(i - gb.lo[0]) * by + (j - gb.lo[1])) * bz + (k - gb.lo[2]);
+    const T ev[3] = {ex, ey, ez};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int64_t q = c * nb + loc;
+        const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
+        gb.g[q] = gb.g[q] + (double)ev[c] * de;
+    }
+}
+
 // Transposed E update: H̄ += B^T ḡ(Ē, P_E); P_E advanced; gradient accumulated.
 template <typename T>
 __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<T> gb) {
@@ -133,6 +152,26 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T ex = a.E[0][idx], ey = a.E[1][idx], ez = a.E[2][idx];
     const T cx = a.ce[0][idx], cy = a.ce[1][idx], cz = a.ce[2][idx];
+    const int np = a.npml;
+    if (np >= 1 && i >= np && i < nx - np - 1 && j >= np && j < ny - np - 1 && k >= np &&
+        k < nz - np - 1) {
+        // the cell and its +1 neighbours lie in no slab: e_pair without P terms
+        const T ikx = a.cpe.ik[0][i], iky = a.cpe.ik[1][j], ikz = a.cpe.ik[2][k];
+        const T ikx1 = a.cpe.ik[0][i + 1], iky1 = a.cpe.ik[1][j + 1], ikz1 = a.cpe.ik[2][k + 1];
+        const T g0 = cx * iky * ex, g1 = -(cx * ikz * ex), g2 = -(cy * ikx * ey);
+        const T g3 = cy * ikz * ey, g4 = cz * ikx * ez, g5 = -(cz * iky * ez);
+        const T g1n = -(a.ce[0][idx + 1] * ikz1 * a.E[0][idx + 1]);
+        const T g3n = a.ce[1][idx + 1] * ikz1 * a.E[1][idx + 1];
+        const T g0n = a.ce[0][idx + sy] * iky1 * a.E[0][idx + sy];
+        const T g5n = -(a.ce[2][idx + sy] * iky1 * a.E[2][idx + sy]);
+        const T g2n = -(a.ce[1][idx + sx] * ikx1 * a.E[1][idx + sx]);
+        const T g4n = a.ce[2][idx + sx] * ikx1 * a.E[2][idx + sx];
+        a.H[0][idx] = a.H[0][idx] + ((g3 - g3n) + (g5 - g5n));
+        a.H[1][idx] = a.H[1][idx] + ((g1 - g1n) + (g4 - g4n));
+        a.H[2][idx] = a.H[2][idx] + ((g0 - g0n) + (g2 - g2n));
+        if (gb.active) adj_grad_cell(gb, i, j, k, ex, ey, ez);
+        return;
+    }
     const T g0 = e_pair<T, 0, true>(a, i, j, k, ex, cx);
     const T g1 = e_pair<T, 1, true>(a, i, j, k, ex, cx);
     const T g2 = e_pair<T, 2, true>(a, i, j, k, ey, cy);
@@ -161,19 +200,7 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<
     a.H[0][idx] = a.H[0][idx] + (tz3 + ty5);
     a.H[1][idx] = a.H[1][idx] + (tz1 + tx4);
     a.H[2][idx] = a.H[2][idx] + (ty0 + tx2);
-    if (gb.active && i >= gb.lo[0] && i < gb.hi[0] && j >= gb.lo[1] && j < gb.hi[1] &&
-        k >= gb.lo[2] && k < gb.hi[2]) {
-        const int by = gb.hi[1] - gb.lo[1], bz = gb.hi[2] - gb.lo[2];
-        const int64_t nb = (int64_t)(gb.hi[0] - gb.lo[0]) * by * bz;
-        const int64_t loc = ((int64_t)(i - gb.lo[0]) * by + (j - gb.lo[1])) * bz + (k - gb.lo[2]);
-        const T ev[3] = {ex, ey, ez};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const int64_t q = c * nb + loc;
-            const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
-            gb.g[q] = gb.g[q] + (double)ev[c] * de;
-        }
-    }
+    if (gb.active) adj_grad_cell(gb, i, j, k, ex, ey, ez);
 }
 
 // Transposed H update: Ē += F^T ā(H̄, P_H); P_H advanced; then the next seed.
@@ -187,6 +214,29 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed 
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T hx = a.H[0][idx], hy = a.H[1][idx], hz = a.H[2][idx];
+    const int np = a.npml;
+    if (np >= 1 && i > np && i < nx - np && j > np && j < ny - np && k > np && k < nz - np) {
+        // the cell and its -1 neighbours lie in no slab: h_pair without P terms
+        const T ikx = a.cph.ik[0][i], iky = a.cph.ik[1][j], ikz = a.cph.ik[2][k];
+        const T ikx1 = a.cph.ik[0][i - 1], iky1 = a.cph.ik[1][j - 1], ikz1 = a.cph.ik[2][k - 1];
+        const T dm = a.dtm;
+        const T a0 = -(dm * iky * hx), a1 = dm * ikz * hx, a2 = dm * ikx * hy;
+        const T a3 = -(dm * ikz * hy), a4 = -(dm * ikx * hz), a5 = dm * iky * hz;
+        const T a1p = dm * ikz1 * a.H[0][idx - 1];
+        const T a3p = -(dm * ikz1 * a.H[1][idx - 1]);
+        const T a0p = -(dm * iky1 * a.H[0][idx - sy]);
+        const T a5p = dm * iky1 * a.H[2][idx - sy];
+        const T a2p = dm * ikx1 * a.H[1][idx - sx];
+        const T a4p = -(dm * ikx1 * a.H[2][idx - sx]);
+        T ex = a.E[0][idx] + ((a3p - a3) + (a5p - a5));
+        T ey = a.E[1][idx] + ((a1p - a1) + (a4p - a4));
+        T ez = a.E[2][idx] + ((a0p - a0) + (a2p - a2));
+        if (sd.active) add_seed<T>(sd, i, j, k, ex, ey, ez);
+        a.E[0][idx] = ex;
+        a.E[1][idx] = ey;
+        a.E[2][idx] = ez;
+        return;
+    }
     const T a0 = h_pair<T, 0, true>(a, i, j, k, hx);
     const T a1 = h_pair<T, 1, true>(a, i, j, k, hx);
     const T a2 = h_pair<T, 2, true>(a, i, j, k, hy);
