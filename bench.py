@@ -19,7 +19,8 @@ The line also carries ``n2f``: the near-to-far contraction of a 320³ box
 (614,400 face samples x 4 currents x 32 frequencies, complex64) onto 361 x 181
 directions in split-BF16 and TF32 on the tensor cores, timed by CUDA events, with
 its error against the float64 direct sum on every 64th direction.
-It also carries ``adjoint``: the ε-gradient leg at 160×160×96 FP32 (npml 12,
+``fp64`` is the same construction at 384³ in FP64 mode (the FP64 throughput
+figure, 136 B/cell of algorithmic traffic).  It also carries ``adjoint``: the ε-gradient leg at 160×160×96 FP32 (npml 12,
 96×96×16 design box, Jx sheet at 30 GHz, 3000 steps, checkpoints every 100 steps,
 objective Σ|Ex(30 GHz)|² over a 32×32 patch): ``t_grad / t_forward`` by CUDA events,
 and the gradient against central differences (h = 1e-3) at 16 seeded voxels in FP64.
@@ -420,10 +421,42 @@ def run_b200_arm(args, rank, world, local):
     }
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if not args.no_fp64:
+        barrier(world)
+        line["fp64"] = run_fp64_leg(args)
     if not args.no_n2f:
         barrier(world)
         line["n2f"] = run_n2f_leg(args)
     return line
+
+
+# ------------------------------------------------------------------ fp64 leg
+def run_fp64_leg(args):
+    """The same construction in FP64 mode (384³ by default): Mcell/s and the
+    fraction of the HBM roofline from counted bytes per cell (FP64 fields)."""
+    import torch
+
+    size, npml = args.fp64_size, args.npml
+    shape = (size, size, size)
+    g, mon = make_engine(size, npml, np.float64)
+    g.set_epsilon(blocky_eps(shape))
+    for _ in range(3):
+        g.step()
+    torch.cuda.synchronize()
+    k = args.fp64_steps
+    total_ms, per_kernel, _ = run_steps_timed(g, k)
+    ms = total_ms / k
+    cells = size**3
+    bpc = alg_bytes_per_cell(shape, npml, 8, ((2, 1, len(FREQS)),))
+    peak, _ = measured_hbm()
+    achieved = bpc * cells / (ms / 1e3) / 1e9
+    del g, mon
+    torch.cuda.empty_cache()
+    return {"workload": f"yee_cpml_{size}^3_fp64_npml{npml}_blocky_eps_jx_point_zdft4",
+            "value": round(cells * k / (total_ms / 1e3) / 1e6, 1), "unit": "Mcell/s",
+            "steps": k, "ms_per_step": round(ms, 4), "alg_bytes_per_cell": round(bpc, 3),
+            "achieved_gbs": round(achieved, 1), "frac": round(achieved / peak, 4),
+            "ms_per_launch": {kk: round(v, 4) for kk, v in per_kernel.items()}}
 
 
 # --------------------------------------------------------------- adjoint leg
@@ -661,7 +694,10 @@ def main(argv=None):
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint-gradient leg (t_grad / t_forward, FD check)")
     ap.add_argument("--no-n2f", action="store_true", help="skip the near-to-far contraction leg")
-    ap.add_argument("--only", choices=("n2f", "adjoint"),
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 throughput leg")
+    ap.add_argument("--fp64-size", type=int, default=384)
+    ap.add_argument("--fp64-steps", type=int, default=100)
+    ap.add_argument("--only", choices=("n2f", "adjoint", "fp64"),
                     help="run one auxiliary leg alone and print its object (profiling)")
     ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
     ap.add_argument("--n2f-freqs", type=int, default=32)
@@ -682,7 +718,7 @@ def main(argv=None):
         return 0
     rank, world, local = dist_setup(args.gpus)
     if args.only:
-        res = run_n2f_leg(args) if args.only == "n2f" else run_adjoint_leg(args)
+        res = {"n2f": run_n2f_leg, "adjoint": run_adjoint_leg, "fp64": run_fp64_leg}[args.only](args)
         if rank == 0:
             print(json.dumps({args.only: res}), flush=True)
         return 0
