@@ -184,6 +184,13 @@ int fdtd_farfield(const fdtd_box *box, const double *acc, int32_t fi, double dl,
                   double k_wave, double eta0, const double *obs_xyz, int32_t n_obs,
                   double *nl_scratch, double *eh, void *stream);
 
+/* Second stage alone: far E, H at n_obs points (float64 xyz, metres) from
+ * NL[n_obs][6] = (Nx, Ny, Nz, Lx, Ly, Lz), complex64 (nl_dtype FDTD_F32) or
+ * complex128 (FDTD_F64); eh[n_obs][6] complex128.  Replaces farfield_nl_to_eh
+ * (dft_farfield.cl:559-635), with the kernel's sign. */
+int fdtd_farfield_eh(const void *nl, int32_t nl_dtype, const double *obs_xyz, int32_t n_obs,
+                     double k_wave, double eta0, double *eh, void *stream);
+
 /* ---- near-to-far contraction on the tensor cores ------------------------ */
 /* NL[f][o][6] = (Nx, Ny, Nz, Lx, Ly, Lz)(r̂_o, f) = Σ_faces Σ_{p,q}
  * e^{+j 2π f r̂_o·r'_{pq}/c0} cur[f][p][q][c], the surface sums that

@@ -118,6 +118,8 @@ SIGNATURES = {
     "fdtd_profile_steps": (c_int32, [c_int32]),
     "fdtd_profile_read": (c_int32, [POINTER(c_double), POINTER(c_int32)]),
     "fdtd_launch_count": (c_int64, []),
+    "fdtd_farfield_eh": (c_int32, [c_void_p, c_int32, c_void_p, c_int32, c_double, c_double,
+                                   c_void_p, c_void_p]),
     "fdtd_n2f_workspace": (c_int32, [POINTER(N2FFace), c_int32, c_int32, c_int32, c_int32,
                                      POINTER(c_uint64)]),
     "fdtd_n2f_contract": (c_int32, [POINTER(N2FFace), c_int32, c_int32, c_void_p, c_int32,

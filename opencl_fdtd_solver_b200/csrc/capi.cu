@@ -25,6 +25,8 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
                             double k_wave, double eta0, const double *obs, int n_obs,
                             double *nl, double *eh, cudaStream_t st);
 int read_fused_error(int reset);
+cudaError_t launch_farfield_eh(const void *nl, int nl_f64, const double *obs, int n_obs,
+                               double k_wave, double eta0, double *eh, cudaStream_t st);
 void profile_enable(bool on);
 cudaError_t profile_read(double ms[4], int *steps);
 struct MatScalars {
@@ -678,6 +680,18 @@ int fdtd_n2f_contract(const fdtd_n2f_face *faces, int32_t nfaces, int32_t cur_dt
     if ((e = fdtd::n2f::launch_contract(mode, P, nfreq, st)) != cudaSuccess)
         return cuda_status(e, "n2f_contract");
     return cuda_status(fdtd::n2f::launch_combine(P, nfreq, (float2 *)nl, st), "n2f_combine");
+}
+
+int fdtd_farfield_eh(const void *nl, int32_t nl_dtype, const double *obs_xyz, int32_t n_obs,
+                     double k_wave, double eta0, double *eh, void *stream) {
+    if (!nl || !obs_xyz || !eh) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    if (n_obs <= 0) return fail(FDTD_ERR_INVALID, "n_obs must be positive, got %d", n_obs);
+    if (nl_dtype != FDTD_F32 && nl_dtype != FDTD_F64)
+        return fail(FDTD_ERR_INVALID, "nl_dtype must be FDTD_F32 or FDTD_F64, got %d", nl_dtype);
+    if (!(k_wave >= 0) || !(eta0 > 0)) return fail(FDTD_ERR_INVALID, "k_wave, eta0 must be positive");
+    return cuda_status(fdtd::launch_farfield_eh(nl, nl_dtype == FDTD_F64, obs_xyz, n_obs, k_wave,
+                                                eta0, eh, (cudaStream_t)stream),
+                       "farfield_eh");
 }
 
 }  // extern "C"

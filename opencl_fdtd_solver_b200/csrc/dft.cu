@@ -247,7 +247,9 @@ __global__ void __launch_bounds__(FF_THREADS)
     }
 }
 
-__global__ void k_farfield_eh(const double2 *nl, const double *obs, int n_obs, double k_wave,
+// NL may be complex128 (the direct sums) or complex64 (the tensor-core contraction).
+template <typename NT>
+__global__ void k_farfield_eh(const NT *nl, const double *obs, int n_obs, double k_wave,
                               double eta0, double2 *eh) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_obs) return;
@@ -257,8 +259,9 @@ __global__ void k_farfield_eh(const double2 *nl, const double *obs, int n_obs, d
     const double rh[3] = {ox / r, oy / r, oz / r};
     double2 N[3], L[3];
     for (int c = 0; c < 3; ++c) {
-        N[c] = nl[6 * (int64_t)p + c];
-        L[c] = nl[6 * (int64_t)p + 3 + c];
+        const NT n = nl[6 * (int64_t)p + c], l = nl[6 * (int64_t)p + 3 + c];
+        N[c] = make_double2((double)n.x, (double)n.y);
+        L[c] = make_double2((double)l.x, (double)l.y);
     }
     double sn, cs;
     sincos(k_wave * r, &sn, &cs);
@@ -383,9 +386,22 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
                                                 dl, k_wave, obs, n_obs,
                                                 reinterpret_cast<double2 *>(nl));
     count_launches(1);
-    k_farfield_eh<<<(n_obs + 127) / 128, 128, 0, st>>>(reinterpret_cast<const double2 *>(nl),
+    k_farfield_eh<double2><<<(n_obs + 127) / 128, 128, 0, st>>>(reinterpret_cast<const double2 *>(nl),
                                                        obs, n_obs, k_wave, eta0,
                                                        reinterpret_cast<double2 *>(eh));
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_farfield_eh(const void *nl, int nl_f64, const double *obs, int n_obs,
+                               double k_wave, double eta0, double *eh, cudaStream_t st) {
+    const unsigned nb = (unsigned)((n_obs + 127) / 128);
+    if (nl_f64)
+        k_farfield_eh<double2><<<nb, 128, 0, st>>>(reinterpret_cast<const double2 *>(nl), obs, n_obs,
+                                                   k_wave, eta0, reinterpret_cast<double2 *>(eh));
+    else
+        k_farfield_eh<float2><<<nb, 128, 0, st>>>(reinterpret_cast<const float2 *>(nl), obs, n_obs,
+                                                  k_wave, eta0, reinterpret_cast<double2 *>(eh));
     count_launches(1);
     return cudaGetLastError();
 }

@@ -514,3 +514,54 @@ def test_launch_counter_and_step_profile(cuda):
     assert all(v > 0 for v in ms)
     # shell H, interior, plane DFT of the interior, shell E per step
     assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
+
+
+def test_medium_config_sphere_box_farfield(cuda):
+    """The medium configuration, shortened to 200 steps: 256³ FP32, npml 12, εr = 4
+    sphere of radius 40 cells, rim-tapered Jx sheet at z = npml + 8 trimmed out of
+    the PML, Gaussian-modulated sine, a closed 6-face DFT box (half-width 44 cells)
+    at 8 frequencies, far field on a 181 (θ) x 91 (φ) grid at R = 1 m.  Fields and
+    box DFTs against the C oracle; far fields direct and through the tensor-core
+    contraction against the oracle's float64 transform."""
+    from oracle.dft_oracle import OracleNear2FarMonitor
+
+    n, npml, dl, steps = 256, 12, 1e-3, 200
+    shape = (n, n, n)
+    eps = sphere_eps(shape, n // 2, 40, 4.0)
+    freqs = np.linspace(20e9, 40e9, 8)
+    g, o = both(cuda, shape, dl, npml)
+    g.set_epsilon(eps)
+    o.set_epsilon(eps)
+    z = npml + 8
+
+    def drive(f):
+        f.add_source_Jx(z, gaussian_sine(f.t, 30e9, 20e9), npml, n - npml, npml, n - npml,
+                        rim_taper=True)
+
+    g.add_source(drive)
+    o.add_source(drive)
+    ctr, size = (n // 2 * dl,) * 3, (88 * dl,) * 3
+    mg = cuda.CUDANear2FarMonitor(g, ctr, size, freqs)
+    mo = OracleNear2FarMonitor(o, ctr, size, freqs)
+    g.run(steps)
+    o.run(steps)
+    assert_same(g, o)
+    for fi in range(freqs.size):
+        a = mg.face_dft(fi)
+        for c in FIELDS:
+            b = mo.dft[c][fi]
+            assert np.abs(a[c] - b).max() <= 1e-9 * np.abs(b).max(), (fi, c)
+    th = np.deg2rad(np.linspace(0.0, 180.0, 181))
+    ph = np.deg2rad(np.linspace(0.0, 180.0, 91, endpoint=False))
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    pts = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1).reshape(-1, 3)
+    # get_farfields rounds observation points to the engine dtype (reference
+    # monitors.py:653); the oracle gets the same rounded points
+    pts32 = pts.astype(np.float32).astype(np.float64)
+    for fi in (0, 7):
+        ref = mo.get_farfields(pts32, fi)
+        d = mg.get_farfields(pts, fi)
+        t = mg.get_farfields(pts, fi, method="bf16x3")
+        scale = np.abs(ref).max()
+        assert np.abs(d - ref).max() <= 1e-9 * scale, fi
+        assert np.abs(t - ref).max() <= 5e-5 * scale, fi
