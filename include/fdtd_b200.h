@@ -120,7 +120,9 @@ int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
 /* One full leapfrog step H -> sources -> E: reads E/H, writes E_next/H_next,
  * ψ stripes in place.  The interior box [npml, N-npml)^3 is updated by one
  * single-pass kernel (H and E per plane, one read and one write of each array);
- * the CPML shell around it by per-cell H and E kernels before and after it.
+ * the CPML shell around it by per-cell kernels: its H on a library-owned side
+ * stream (per host thread and device) that overlaps the interior kernel and is
+ * joined back by an event, its E afterwards on the caller's stream.
  * Replaces the whole of OpenCLFDTD.step() up to the monitors
  * (engine.py:724-735): _update_H, the source callbacks' injections, _update_E. */
 int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
@@ -316,7 +318,7 @@ int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int
  * the sums and records CUDA events around every launch of each following
  * fdtd_step on its stream; enable == 0 stops recording.  fdtd_profile_read
  * waits for the recorded events and returns the summed milliseconds per
- * launch, [0] CPML-shell H, [1] interior single-pass kernel, [2] plane DFT of
+ * launch, [0] CPML-shell H (on the side stream, concurrent with [1]), [1] interior single-pass kernel, [2] plane DFT of
  * the interior, [3] CPML-shell E (with sources and DFTs), and the number of
  * steps recorded.  No reference counterpart. */
 int fdtd_profile_steps(int32_t enable);
