@@ -12,7 +12,7 @@
 // K = p, N = (q, c)), and NL_face(o, c) = C(o)·Σ_q v_q(o)·T[o][q][c] is a
 // row-wise reduction of its output.
 //
-// Kernel k_n2f_tc: one CTA per (128-direction tile, face, frequency), 14 warps.
+// Kernel k_n2f_tc: one CTA per (128-direction tile, face, frequency), 6 + 4·NGRP warps.
 //   * warp 0: B producer.  B (currents, N × K) is pre-packed by k_n2f_pack in
 //     the K-major core-matrix layout, one contiguous 16 KB (8 KB) block per
 //     (n tile, K step), and moved with one cp.async.bulk per stage (no tensor
@@ -20,8 +20,8 @@
 //   * warp 1: one thread issues tcgen05.mma (kind::f16 BF16: hi·hi + hi·lo +
 //     lo·hi, or kind::tf32) into a 128 × 256 FP32 accumulator in TMEM,
 //     double-buffered across n tiles (512 columns).
-//   * warps 2-5 and 10-13: A (phases, 128 × K), generated in shared memory per
-//     K step, one direction per thread, the two groups on alternate stages: a
+//   * warps 2-5 and 10 onwards: A (phases, 128 × K), generated in shared memory
+//     per K step, one direction per thread, NGRP groups on interleaved stages: a
 //     float64 rotation times eight (four) precomputed float phases, split into
 //     bf16 hi + lo (or rounded to tf32), written in the K-major core-matrix
 //     layout.
@@ -47,7 +47,8 @@ namespace n2f {
 
 __device__ int g_n2f_error;
 
-constexpr int NTHREADS = 448;  // B loader, MMA issuer, 2 x 4 phase warps, 4 epilogue warps
+constexpr int NGRP = 2;  // phase-generator groups of four warps, on stages g % NGRP
+constexpr int NTHREADS = (6 + 4 * NGRP) * 32;  // B loader, MMA issuer, epilogue, phase groups
 constexpr int MAX_STAGE = 16;
 constexpr double C0 = 299792458.0;
 
@@ -367,26 +368,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             if (last >= 0) drain_bar(smem_u32(&sm->empty[last % NSTAGE]), (last / NSTAGE) & 1);
         }
     } else if ((warp >= 2 && warp < 6) || warp >= 10) {
-        // ---- A producers: phases u_p(o), one row (direction) per thread; two
-        // groups of four warps take the even and the odd stages.
+        // group 0: warps 2-5; group h >= 1: warps 10 + 4(h-1) .. 13 + 4(h-1)
+        // ---- A producers: phases u_p(o), one row (direction) per thread; NGRP
+        // groups of four warps take the stages g with g % NGRP == group.
         // u_{ks*PS + i} = U_ks * w_i with w_i = e^{j2π γ i} (float, exact to an
         // ulp) and U_ks = e^{j2π γ ks PS}, evaluated in float64 at the group's
-        // first stage of each n tile and advanced by a float64 rotation of two K
+        // first stage of each n tile and advanced by a float64 rotation of NGRP K
         // steps after that, so each value carries one float rounding.
-        const int grp = warp >= 10 ? 1 : 0;
-        const int r = tid - (grp ? 320 : 64);  // 0..127
+        const int grp = warp >= 10 ? 1 + (warp - 10) / 4 : 0;
+        const int r = grp ? tid - (320 + 128 * (grp - 1)) : tid - 64;  // 0..127
         const int o = mt * BM + r;
         const bool valid = o < P.n_obs;
         const double gp = valid ? freq * F.pitch * P.dirs[3 * o + F.axis_p] / C0 : 0.0;
         float2 w[C::PS];
 #pragma unroll
         for (int i = 0; i < C::PS; ++i) w[i] = phase_turns(gp, (double)i);
-        const double2 W2 = zphase_turns(gp, (double)(2 * C::PS));
+        const double2 W2 = zphase_turns(gp, (double)(NGRP * C::PS));
         // core-matrix offset of (row r, chunk c): (c*BM/8 + r/8)*128 + (r%8)*16
         const int roff = (r >> 3) * 128 + (r & 7) * 16;
         double2 U = make_double2(1.0, 0.0);
         int prev_ks = -1;
-        for (int g = grp; g < total; g += 2) {
+        for (int g = grp; g < total; g += NGRP) {
             const int s = g % NSTAGE, ks = g % KS;
             if (ks <= prev_ks || prev_ks < 0) U = zphase_turns(gp, (double)(ks * C::PS));
             prev_ks = ks;
