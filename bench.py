@@ -147,7 +147,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """One process per GPU (torchrun's RANK/LOCAL_RANK/WORLD_SIZE); the only
+    collectives are a barrier and a max-reduction of the device time."""
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -158,23 +160,34 @@ def dist_setup(n_gpus):
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, world, local
 
 
 def reduce_max(x, world):
+    """Max of x over the ranks (the job's time is its slowest replica's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_rate(world, cells, steps, max_ms):
+    """Whole-job Mcell/s of `world` replicas that each advanced `cells` cells
+    `steps` steps, timed by the slowest replica."""
+    return world * cells * steps / (max_ms / 1e3) / 1e6
 
 
 def barrier(world):
@@ -326,7 +339,7 @@ def run_b200_arm(args, rank, world, local):
     total_ms = reduce_max(total_ms, world)
     clocks = clk.summary()
     ms_per_step = total_ms / args.steps
-    value = world * cells * args.steps / (total_ms / 1e3) / 1e6
+    value = aggregate_rate(world, cells, args.steps, total_ms)
     fused = g._fused_enabled
 
     item = 4
@@ -372,7 +385,7 @@ def run_b200_arm(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_wall = time.perf_counter() - t0
     e2e_dev_ms = reduce_max(ev0.elapsed_time(ev1), world)
-    e2e_value = world * cells * args.steps / (e2e_dev_ms / 1e3) / 1e6
+    e2e_value = aggregate_rate(world, cells, args.steps, e2e_dev_ms)
     h2d = eps.nbytes  # εr; the coefficients are built on the device
     d2h = dft.nbytes + plane.nbytes
     del g2, mon2
