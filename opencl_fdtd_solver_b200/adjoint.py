@@ -14,7 +14,8 @@ one on top of :class:`CUDAFDTD` without changing the forward path:
   ``fdtd_adjoint_step``); segments are replayed from their checkpoints, newest
   first, with ``E`` captured over the design's edge box each step
   (``fdtd_capture_box``), and the transposed step runs backwards through the segment
-  (``fdtd_adjoint_step``), accumulating ``Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce``
+  (``fdtd_adjoint_step``) on a second stream, concurrently with the replay of the
+  next-older segment (two capture buffers, ordered by events), accumulating ``Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce``
   on the edge box in float64.  The host chain rule through ``ce = dt/(ε0·ε_edge)``
   and the two-cell edge average (reference ``materials.py:28-56``) gives
   ``∂J/∂εr`` per design cell.
@@ -262,13 +263,15 @@ class EpsilonAdjoint:
             raise NotImplementedError("the adjoint gradient needs a lossless grid")
         st = fd.queue.cuda_stream
         N, K = self.n_steps, self.K
+        nseg = len(self._ckpts)
         with torch.cuda.stream(fd.queue):
             Eb, Hb, PE, PH, fields = self._adjoint_buffers()
             phases = _phase_sequence(o.freqs, fd.dt, N, self._t_first)
             ph_dev = torch.from_numpy(np.ascontiguousarray(
                 np.stack([phases.real, phases.imag], -1))).to(fd.device)
             G = torch.zeros((3, *self.box_shape), dtype=torch.float64, device=fd.device)
-            cap = torch.empty((K + 1, 3, *self.box_shape), dtype=fd._tdt, device=fd.device)
+            # two capture buffers: segment s is swept while segment s-1 is replayed
+            cap = torch.empty((2, K + 1, 3, *self.box_shape), dtype=fd._tdt, device=fd.device)
         (a0, a1), (b0, b1) = o.patch
         sd = capi.AdjointSeed(axis=o.axis, index=o.index, a0=a0, a1=a1, b0=b0, b1=b1,
                               comp_mask=o.comp_mask, nfreq=o.freqs.size,
@@ -281,38 +284,75 @@ class EpsilonAdjoint:
         gb.g = G.data_ptr()
         lo = (ctypes.c_int32 * 3)(*[b[0] for b in self.box])
         hi = (ctypes.c_int32 * 3)(*[b[1] for b in self.box])
-        cap_stride = cap[0].numel() * cap.element_size()
+        slot = cap[0, 0].numel() * cap.element_size()
+        buf = cap[0].numel() * cap.element_size()
         cap0 = cap.data_ptr()
         grid, cpml = fd._grid, fd._cpml_base
         Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb])
+        # the reverse sweep runs on its own stream, concurrently with the replay
+        # of the next-older segment on the engine's stream
+        adj = torch.cuda.Stream(device=fd.device)
+        ast = adj.cuda_stream
+        ready = torch.cuda.Event()
+        ready.record(fd.queue)
+        adj.wait_event(ready)
         sd.phase = ph0 + (N - 1) * ph_stride
-        capi.run("fdtd_adjoint_seed_add", grid, Ebp, sd, st)
+        capi.run("fdtd_adjoint_seed_add", grid, Ebp, sd, ast)
+
+        def replay(seg):
+            """Replay segment seg from its checkpoint, capturing E over the edge box;
+            yields after each unit of work it enqueued on the engine's stream."""
+            base = cap0 + (seg % 2) * buf
+            fd.load_state(self._ckpts[seg])
+            for m in range(min(N, (seg + 1) * K) - seg * K + 1):
+                if m > 0:
+                    fd.step()
+                Ep = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in fd._E])
+                capi.run("fdtd_capture_box", grid, Ep, lo, hi, base + m * slot, st)
+                yield
+
         saved = fd._monitors
         fd._monitors = []
         par = 0
+        replayed, swept = {}, {}
         try:
-            for s in range(len(self._ckpts) - 1, -1, -1):
+            for _ in replay(nseg - 1):
+                pass
+            replayed[nseg - 1] = torch.cuda.Event()
+            replayed[nseg - 1].record(fd.queue)
+            for s in range(nseg - 1, -1, -1):
+                adj.wait_event(replayed[s])
+                gen = None
+                if s >= 1:
+                    if s + 1 in swept:  # the buffer segment s-1 fills was swept as s+1
+                        fd.queue.wait_event(swept[s + 1])
+                    gen = replay(s - 1)
                 n0 = s * K
                 n1 = min(N, n0 + K)
-                fd.load_state(self._ckpts[s])
-                for m in range(n1 - n0 + 1):
-                    if m > 0:
-                        fd.step()
-                    Ep = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in fd._E])
-                    capi.run("fdtd_capture_box", grid, Ep, lo, hi, cap0 + m * cap_stride, st)
+                base = cap0 + (s % 2) * buf
                 for n in range(n1 - 1, n0 - 1, -1):
-                    gb.e_next = cap0 + (n + 1 - n0) * cap_stride
-                    gb.e_prev = cap0 + (n - n0) * cap_stride
+                    if gen is not None:
+                        next(gen, None)
+                    gb.e_next = base + (n + 1 - n0) * slot
+                    gb.e_prev = base + (n - n0) * slot
                     if n >= 1:
                         sd.phase = ph0 + (n - 1) * ph_stride
                         seed_arg = ctypes.byref(sd)
                     else:
                         seed_arg = None
-                    capi.run("fdtd_adjoint_step", grid, fields[par], cpml, gb, seed_arg, st)
+                    capi.run("fdtd_adjoint_step", grid, fields[par], cpml, gb, seed_arg, ast)
                     par ^= 1
+                if gen is not None:
+                    for _ in gen:
+                        pass
+                    replayed[s - 1] = torch.cuda.Event()
+                    replayed[s - 1].record(fd.queue)
+                swept[s] = torch.cuda.Event()
+                swept[s].record(adj)
         finally:
             fd._monitors = saved
-        fd.queue.synchronize()
+            adj.synchronize()
+            fd.queue.synchronize()
         self._adjoint_state = (Eb, Hb)
         g_edges = G.cpu().numpy()
         return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)
