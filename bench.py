@@ -268,8 +268,11 @@ def run_reference_arm(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(args.size**3 / value / 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"yee_cpml_{args.size}^3_fp32_npml{args.npml}_blocky_eps",
-                   "cpu": True},
+        "config": {"workload": f"yee_cpml_{args.size}^3_fp32_npml{args.npml}_blocky_eps_jx_point_zdft4",
+                   "grid": [args.size] * 3, "npml": args.npml, "eps_seed": 1234,
+                   "cpu": True,
+                   "note": "the reference's Yee/CPML and source kernels on the host cores; the "
+                           "plane DFT has no reference kernel and is not part of this arm's step"},
         "cpu_baseline": {"value": round(value, 2), "unit": "Mcell/s", "cores": thr, "kind": kind,
                          "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "Mcell/s", "h2d_bytes_per_step": 0,
