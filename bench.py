@@ -695,6 +695,63 @@ def run_n2f_leg(args):
     }
 
 
+# ----------------------------------------------------------- host-monitor leg
+def run_host_monitor_leg(args):
+    """Per-step cost of the reference's host Huygens-box monitor on 256³ FP32
+    (npml 12, box half-width 44 cells, one frequency): this package's
+    ``NumPyNear2FarMonitor`` reading only its face slabs (``host_regions``)
+    against the same monitor reading six full volumes per step, beside the bare
+    step.  Wall-clock per step (the monitor runs on the host between steps)."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import CUDAFDTD, NumPyNear2FarMonitor
+
+    size, npml, dl, half = 256, 12, 1e-3, 44
+    shape = (size,) * 3
+    c = size // 2
+    ctr = (c * dl,) * 3
+    box = (2 * half * dl,) * 3
+
+    class FullReads(NumPyNear2FarMonitor):
+        host_regions = None
+
+    def engine(mon_cls):
+        g = CUDAFDTD(shape, dl, npml=npml)
+        g.add_source(lambda f: f.add_source_Jx(c, gaussian_sine(f.t), i0=c, i1=c + 1, j0=c,
+                                               j1=c + 1))
+        m = mon_cls(g, ctr, box, ADJ_FREQ) if mon_cls else None
+        return g, m
+
+    def per_step(g, k):
+        for _ in range(3):
+            g.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            g.step()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / k * 1e3
+
+    out = {"workload": f"host_n2f_monitor_{size}^3_fp32_npml{npml}_box{2 * half + 1}",
+           "unit": "ms/step"}
+    g, _ = engine(None)
+    out["bare_step_ms"] = round(per_step(g, 200), 4)
+    del g
+    g, m = engine(NumPyNear2FarMonitor)
+    out["windowed_ms"] = round(per_step(g, 100), 4)
+    cells = sum((a1 - a0) * (b1 - b0) * (c1 - c0)
+                for (a0, a1), (b0, b1), (c0, c1) in m.host_regions())
+    out["windowed_d2h_bytes_per_step"] = 6 * 4 * cells
+    del g, m
+    g, m = engine(FullReads)
+    out["full_reads_ms"] = round(per_step(g, 10), 4)
+    out["full_reads_d2h_bytes_per_step"] = 6 * 4 * size**3
+    del g, m
+    torch.cuda.empty_cache()
+    out["speedup"] = round(out["full_reads_ms"] / out["windowed_ms"], 2)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -713,7 +770,7 @@ def main(argv=None):
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 throughput leg")
     ap.add_argument("--fp64-size", type=int, default=384)
     ap.add_argument("--fp64-steps", type=int, default=100)
-    ap.add_argument("--only", choices=("n2f", "adjoint", "fp64"),
+    ap.add_argument("--only", choices=("n2f", "adjoint", "fp64", "host_monitor"),
                     help="run one auxiliary leg alone and print its object (profiling)")
     ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
     ap.add_argument("--n2f-freqs", type=int, default=32)
@@ -734,7 +791,8 @@ def main(argv=None):
         return 0
     rank, world, local = dist_setup(args.gpus)
     if args.only:
-        res = {"n2f": run_n2f_leg, "adjoint": run_adjoint_leg, "fp64": run_fp64_leg}[args.only](args)
+        res = {"n2f": run_n2f_leg, "adjoint": run_adjoint_leg, "fp64": run_fp64_leg,
+               "host_monitor": run_host_monitor_leg}[args.only](args)
         if rank == 0:
             print(json.dumps({args.only: res}), flush=True)
         return 0

@@ -298,6 +298,29 @@ int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fd
                       const fdtd_grad_box *gb, const fdtd_adjoint_seed *next_seed,
                       void *stream);
 
+/* ---- host reads of sub-boxes --------------------------------------------- */
+
+#define FDTD_MAX_REGIONS 32     /* boxes per fdtd_read_regions call            */
+
+/* Half-open cell box [lo, hi) of one field. */
+typedef struct {
+    int32_t lo[3], hi[3];
+} fdtd_region;
+
+/* Copy the cells of nreg boxes of one (nx, ny, nz) field to host memory: the
+ * boxes are packed one after another, each in C order, into the device buffer
+ * `staging` by one gather launch, then moved to `host` by one device-to-host
+ * copy.  Both buffers hold Σ box cells elements of the field dtype.  The copy
+ * is asynchronous on `stream` when `host` is pinned; the caller synchronises
+ * the stream before reading `host`.  Empty boxes (lo == hi on an axis) are
+ * allowed and contribute nothing.  Replaces, for the listed boxes only, the
+ * reference's full-volume read of a field (_read_field, engine.py:747-751,
+ * behind the Ex…Hz properties, engine.py:767-789), which host monitors such as
+ * NumPyNear2FarMonitor.__call__ (monitors.py:229-295) issue every step. */
+int fdtd_read_regions(const void *field, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                      const fdtd_region *regions, int32_t nreg, void *staging, void *host,
+                      void *stream);
+
 /* ---- materials ----------------------------------------------------------- */
 
 /* Yee-edge coefficients from cell-centred εr (and conductivity σ in S/m, may

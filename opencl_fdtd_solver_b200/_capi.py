@@ -25,6 +25,7 @@ FDTD_F64 = 1
 FDTD_MAX_SOURCES = 8
 FDTD_MAX_PLANES = 4
 FDTD_MAX_FREQS = 64
+FDTD_MAX_REGIONS = 32
 FDTD_NOALLOC_MAX_FACE = 1024 * 256
 FDTD_SRC_JX = 0
 FDTD_SRC_EX = 1
@@ -84,6 +85,10 @@ class GradBox(Structure):
                 ("e_prev", c_void_p), ("g", c_void_p)]
 
 
+class Region(Structure):
+    _fields_ = [("lo", c_int32 * 3), ("hi", c_int32 * 3)]
+
+
 class N2FFace(Structure):
     _fields_ = [("normal", c_int32), ("np", c_int32), ("nq", c_int32), ("pad_", c_int32),
                 ("x_n", c_double), ("o_p", c_double), ("o_q", c_double), ("pitch", c_double),
@@ -109,6 +114,8 @@ SIGNATURES = {
                                 c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "fdtd_capture_box": (c_int32, [POINTER(Grid), POINTER(c_void_p), POINTER(c_int32),
                                    POINTER(c_int32), c_void_p, c_void_p]),
+    "fdtd_read_regions": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_int32,
+                                    POINTER(Region), c_int32, c_void_p, c_void_p, c_void_p]),
     "fdtd_adjoint_seed_add": (c_int32, [POINTER(Grid), POINTER(c_void_p), POINTER(AdjointSeed),
                                         c_void_p]),
     "fdtd_adjoint_step": (c_int32, [POINTER(Grid), POINTER(AdjointFields), POINTER(Cpml),

@@ -12,6 +12,7 @@
 #include "yee_launch.cuh"
 #include "adjoint.cuh"
 #include "n2f.cuh"
+#include "hostio.cuh"
 
 namespace fdtd {
 template <typename T>
@@ -525,6 +526,45 @@ int fdtd_capture_box(const fdtd_grid *g, const void *const E[3], const int32_t l
     return cuda_status(fdtd::launch_capture<double>(g->ny, g->nz, (const double *const *)E, lo,
                                                     hi, (double *)out, st),
                        "capture_box");
+}
+
+int fdtd_read_regions(const void *field, int32_t dtype, int32_t nx, int32_t ny, int32_t nz,
+                      const fdtd_region *regions, int32_t nreg, void *staging, void *host,
+                      void *stream) {
+    if (dtype != FDTD_F32 && dtype != FDTD_F64) return fail(FDTD_ERR_INVALID, "dtype %d", dtype);
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return fail(FDTD_ERR_INVALID, "shape (%d, %d, %d)", nx, ny, nz);
+    if (nreg < 0 || nreg > FDTD_MAX_REGIONS)
+        return fail(FDTD_ERR_INVALID, "%d regions (at most %d)", nreg, FDTD_MAX_REGIONS);
+    if (nreg > 0 && !regions) return fail(FDTD_ERR_INVALID, "regions is NULL");
+    const int dims[3] = {nx, ny, nz};
+    fdtd::RegionList r;
+    memset(&r, 0, sizeof(r));
+    r.n = nreg;
+    r.off[0] = 0;
+    for (int q = 0; q < nreg; ++q) {
+        int64_t cells = 1;
+        for (int a = 0; a < 3; ++a) {
+            const int32_t lo = regions[q].lo[a], hi = regions[q].hi[a];
+            if (lo < 0 || hi > dims[a] || lo > hi)
+                return fail(FDTD_ERR_INVALID, "region %d axis %d: [%d, %d) outside [0, %d)", q,
+                            a, lo, hi, dims[a]);
+            r.lo[q][a] = lo;
+            r.ext[q][a] = hi - lo;
+            cells *= hi - lo;
+        }
+        r.off[q + 1] = r.off[q] + cells;
+    }
+    if (r.off[nreg] == 0) return FDTD_OK;
+    if (!field || !staging || !host) return fail(FDTD_ERR_INVALID, "NULL buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == FDTD_F32)
+        return cuda_status(fdtd::launch_read_regions<float>((const float *)field, ny, nz, r,
+                                                            (float *)staging, host, st),
+                           "read_regions");
+    return cuda_status(fdtd::launch_read_regions<double>((const double *)field, ny, nz, r,
+                                                         (double *)staging, host, st),
+                       "read_regions");
 }
 
 int fdtd_adjoint_seed_add(const fdtd_grid *g, void *const Ebar[3], const fdtd_adjoint_seed *seed,

@@ -6,7 +6,9 @@ Reference contract (``opencl_fdtd_solver/engine.py``):
 * ``set_epsilon(eps, sigma_array=None)``: ``engine.py:212-254``
 * ``add_source_Jx`` / ``add_source_Ex``: ``engine.py:448-538``
 * ``step`` / ``run`` (H → sources at t+dt/2 → E → t+=dt → monitors): ``engine.py:724-744``
-* host field reads ``Ex…Hz`` and ``read_point``: ``engine.py:746-789``
+* host field reads ``Ex…Hz`` and ``read_point``: ``engine.py:746-789``; sub-box reads
+  (``read_region``, ``read_plane``, ``host_window``) move only the cells a host
+  monitor needs (``fdtd_read_regions``)
 
 Design.  Torch tensors own every device buffer; the kernels are reached only
 through the C ABI of ``libfdtd_b200.so`` (``_capi.py``).  A step normally runs as
@@ -26,6 +28,7 @@ constructor raises.
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import logging
 import warnings
@@ -109,6 +112,9 @@ class CUDAFDTD(SourceMonitorMixin):
         self._sources = []
         self._monitors = []
         self._fused_enabled = bool(fused)
+        self._read_window = None    # boxes served by Ex…Hz inside host_window()
+        self._mirror = {}           # field name -> full-shape host array (windowed reads)
+        self._hostio = None         # (device staging, pinned host) buffers of fdtd_read_regions
 
         mem_device = ctx.devices[0] if (ctx is not None and hasattr(ctx, "devices")) else None
         torch = _torch()
@@ -425,7 +431,12 @@ class CUDAFDTD(SourceMonitorMixin):
         self.t += self.dt
         self.step_num += 1
         for mon in self._monitors:
-            mon(self)
+            regs = getattr(mon, "host_regions", None)
+            if regs is None:
+                mon(self)
+            else:
+                with self.host_window(regs() if callable(regs) else regs):
+                    mon(self)
 
     def _swap(self):
         self._E, self._En = self._En, self._E
@@ -485,9 +496,116 @@ class CUDAFDTD(SourceMonitorMixin):
         return self._E[k] if k < 3 else self._H[k - 3]
 
     def _read_field(self, name):
+        if self._read_window is not None:
+            return self._window_read(name, self._read_window)
         t = self.field_tensor(name)
         self.queue.synchronize()
         return t.cpu().numpy()
+
+    # ---------------------------------------------------- sub-box host reads
+    def _norm_regions(self, regions):
+        """Validated half-open boxes ``((i0, i1), (j0, j1), (k0, k1))``."""
+        dims = (self.Nx, self.Ny, self.Nz)
+        out = []
+        for r in regions:
+            box = tuple((int(a), int(b)) for a, b in r)
+            if len(box) != 3 or any(not 0 <= a <= b <= n for (a, b), n in zip(box, dims)):
+                raise ValueError(f"region {r!r} is not a half-open box inside {dims}")
+            out.append(box)
+        return out
+
+    def _gather(self, name, boxes):
+        """Host views of ``boxes`` of field ``name``, valid until the next gather.
+
+        One ``fdtd_read_regions`` call (one gather launch plus one device-to-host
+        copy into a pinned buffer) per ``FDTD_MAX_REGIONS`` boxes, then one stream
+        synchronisation.
+        """
+        torch = _torch()
+        t = self.field_tensor(name)
+        sizes = [(i1 - i0) * (j1 - j0) * (k1 - k0) for (i0, i1), (j0, j1), (k0, k1) in boxes]
+        total = int(sum(sizes))
+        if self._hostio is None or self._hostio[0].numel() < total:
+            n = 1 << max(16, (max(total, 1) - 1).bit_length())
+            with torch.cuda.stream(self.queue):
+                dev = torch.empty(n, dtype=t.dtype, device=self.device)
+            self._hostio = (dev, torch.empty(n, dtype=t.dtype, pin_memory=True))
+        dev, pin = self._hostio
+        item = t.element_size()
+        dt = capi.FDTD_F64 if self.dtype == np.float64 else capi.FDTD_F32
+        off = 0
+        for c in range(0, len(boxes), capi.FDTD_MAX_REGIONS):
+            chunk = boxes[c:c + capi.FDTD_MAX_REGIONS]
+            regs = (capi.Region * len(chunk))()
+            for q, box in enumerate(chunk):
+                regs[q].lo[:] = [a for a, _ in box]
+                regs[q].hi[:] = [b for _, b in box]
+            capi.run("fdtd_read_regions", t.data_ptr(), dt, self.Nx, self.Ny, self.Nz, regs,
+                     len(chunk), dev.data_ptr() + off * item, pin.data_ptr() + off * item,
+                     self.queue.cuda_stream)
+            off += sum(sizes[c:c + capi.FDTD_MAX_REGIONS])
+        self.queue.synchronize()
+        flat = pin.numpy()
+        out, off = [], 0
+        for box, n in zip(boxes, sizes):
+            out.append(flat[off:off + n].reshape([b - a for a, b in box]))
+            off += n
+        return out
+
+    def read_region(self, name, lo, hi):
+        """Host copy of field ``name`` over the half-open box ``[lo, hi)``.
+
+        Only the box crosses to the host (gathered on the device, then one copy
+        through pinned memory), instead of the whole volume that the ``Ex…Hz``
+        properties move (``engine.py:747-751``).
+        """
+        FIELD_NAMES.index(name)
+        box = self._norm_regions([tuple(zip(lo, hi))])
+        return self._gather(name, box)[0].copy()
+
+    def read_plane(self, name, axis, index):
+        """Host copy of one plane of field ``name``: ``axis`` in ``'x'``/``'y'``/``'z'`` or 0-2."""
+        a = {"x": 0, "y": 1, "z": 2}.get(axis, axis)
+        if a not in (0, 1, 2):
+            raise ValueError(f"axis must be x, y, z or 0-2, got {axis!r}")
+        dims = (self.Nx, self.Ny, self.Nz)
+        index = int(index)
+        if not 0 <= index < dims[a]:
+            raise ValueError(f"plane index {index} outside [0, {dims[a]})")
+        lo = [0, 0, 0]
+        hi = list(dims)
+        lo[a], hi[a] = index, index + 1
+        return self.read_region(name, lo, hi).reshape([d for q, d in enumerate(dims) if q != a])
+
+    def _window_read(self, name, boxes):
+        mirror = self._mirror.get(name)
+        if mirror is None:
+            mirror = self._mirror[name] = np.zeros((self.Nx, self.Ny, self.Nz), self.dtype)
+        for box, part in zip(boxes, self._gather(name, boxes)):
+            mirror[tuple(slice(a, b) for a, b in box)] = part
+        view = mirror.view()
+        view.flags.writeable = False
+        return view
+
+    @contextlib.contextmanager
+    def host_window(self, regions):
+        """Serve ``Ex…Hz`` reads inside the block from the listed boxes only.
+
+        ``regions`` is a list of half-open boxes ``((i0, i1), (j0, j1), (k0, k1))``.
+        Within the block a field property returns a read-only ``(Nx, Ny, Nz)``
+        array that holds the current values inside the boxes (values elsewhere
+        are unspecified), and only the boxes cross to the host.  ``step()`` opens
+        this window around each monitor that declares ``host_regions`` (a list of
+        boxes, or a callable returning one), so a host monitor that reads a few
+        planes per step moves those planes rather than six volumes.  Reads
+        outside the block are full reads again.
+        """
+        boxes = self._norm_regions(regions)
+        prev, self._read_window = self._read_window, boxes
+        try:
+            yield self
+        finally:
+            self._read_window = prev
 
     def _write_field(self, name, value):
         torch = _torch()

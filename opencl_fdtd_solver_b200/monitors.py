@@ -9,6 +9,10 @@ x0,x1,y0,y1,z0,z1 (``:396-412``), per-step phase recurrence (``:456-459, 571-584
 slice per frequency); a scalar ``freq`` keeps the reference form.  Far fields use
 the reference kernel's sign ``η·N⊥ − r̂×L`` (``dft_farfield.cl:617``).
 
+``NumPyNear2FarMonitor`` is the reference's host monitor (``monitors.py:186-380``):
+it accumulates from the engine's host field reads, which ``CUDAFDTD`` restricts
+to the face slabs the monitor declares.
+
 ``CUDAPlaneDFTMonitor`` has no reference class: a running DFT of chosen field
 components on one grid plane, accumulated inside the E-update kernel (no extra
 pass over the fields), with the same phase convention (E at the step time, H half
@@ -33,6 +37,43 @@ def _torch():
     import torch
 
     return torch
+
+
+def _box_struct(box, offsets, n_face, nfreq):
+    b = capi.Box()
+    b.ix0, b.ix1, b.iy0, b.iy1, b.iz0, b.iz1 = box
+    for q in range(6):
+        b.off[q] = offsets[q]
+    b.n_face = n_face
+    b.nfreq = nfreq
+    return b
+
+
+def _device_farfields(fdtd, cbox, acc, fi, freq, pts):
+    """Far E, H ``(n_obs, 6)`` complex128 from face accumulators ``acc`` (device,
+    ``(6, nfreq, n_face, 2)`` float64) with the float64 surface-sum kernel."""
+    torch = _torch()
+    n_obs = int(pts.shape[0])
+    q = fdtd.queue
+    with torch.cuda.stream(q):
+        obs = torch.from_numpy(pts.astype(np.float64)).to(fdtd.device)
+        nl = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=fdtd.device)
+        eh = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=fdtd.device)
+    k_wave = 2.0 * np.pi * freq / C0
+    capi.run("fdtd_farfield", cbox, acc.data_ptr(), int(fi), float(fdtd.dl), k_wave, float(ETA0),
+             obs.data_ptr(), n_obs, nl.data_ptr(), eh.data_ptr(), q.cuda_stream)
+    q.synchronize()
+    h = eh.cpu().numpy()
+    return (h[..., 0] + 1j * h[..., 1]).astype(np.complex128)
+
+
+def _obs_array(obs_points, dtype):
+    pts = np.asarray(obs_points, dtype=dtype)
+    if pts.ndim == 1:
+        pts = pts.reshape(1, 3)
+    if pts.ndim != 2 or pts.shape[1] != 3:
+        raise ValueError("obs_points must be (n,3) or (3,)")
+    return pts
 
 
 class _PhaseTable:
@@ -189,13 +230,8 @@ class CUDANear2FarMonitor:
         self.n_face_samples = int(sum(self._face_counts))
         self._dtype = fdtd.dtype
         self._acc_complex_dtype = fdtd.accreal_complex_dtype
-        b = capi.Box()
-        b.ix0, b.ix1, b.iy0, b.iy1, b.iz0, b.iz1 = self._box
-        for q in range(6):
-            b.off[q] = self._face_offsets[q]
-        b.n_face = self.n_face_samples
-        b.nfreq = self.freqs.size
-        self._cbox = b
+        self._cbox = _box_struct(self._box, self._face_offsets, self.n_face_samples,
+                                 self.freqs.size)
         with torch.cuda.stream(fdtd.queue):
             self.acc = torch.zeros((6, self.freqs.size, self.n_face_samples, 2),
                                    dtype=torch.float64, device=fdtd.device)
@@ -236,36 +272,16 @@ class CUDANear2FarMonitor:
         """
         if method != "direct":
             return self._farfields_contract(obs_points, freq_index, method)
-        torch = _torch()
-        pts = np.asarray(obs_points, dtype=self._dtype)
-        if pts.ndim == 1:
-            pts = pts.reshape(1, 3)
-        if pts.ndim != 2 or pts.shape[1] != 3:
-            raise ValueError("obs_points must be (n,3) or (3,)")
+        pts = _obs_array(obs_points, self._dtype)
         fi = self._fi(freq_index)
-        n_obs = int(pts.shape[0])
-        q = self.fdtd.queue
-        with torch.cuda.stream(q):
-            obs = torch.from_numpy(pts.astype(np.float64)).to(self.fdtd.device)
-            nl = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=self.fdtd.device)
-            eh = torch.empty((n_obs, 6, 2), dtype=torch.float64, device=self.fdtd.device)
-        k_wave = 2.0 * np.pi * float(self.freqs[fi]) / C0
-        capi.run("fdtd_farfield", self._cbox, self.acc.data_ptr(), fi, float(self.dl), k_wave,
-                 float(ETA0), obs.data_ptr(), n_obs, nl.data_ptr(), eh.data_ptr(), q.cuda_stream)
-        q.synchronize()
-        h = eh.cpu().numpy()
-        return (h[..., 0] + 1j * h[..., 1]).astype(np.complex128)
+        return _device_farfields(self.fdtd, self._cbox, self.acc, fi, float(self.freqs[fi]), pts)
 
     def _farfields_contract(self, obs_points, freq_index, method):
         from .n2f import box_faces, near2far_contract
 
         torch = _torch()
         # points in the engine dtype, as the direct path and the reference do
-        pts = np.asarray(obs_points, dtype=self._dtype).astype(np.float64)
-        if pts.ndim == 1:
-            pts = pts.reshape(1, 3)
-        if pts.ndim != 2 or pts.shape[1] != 3:
-            raise ValueError("obs_points must be (n,3) or (3,)")
+        pts = _obs_array(obs_points, self._dtype).astype(np.float64)
         fi = self._fi(freq_index)
         q = self.fdtd.queue
         faces = box_faces(self)
@@ -365,6 +381,188 @@ class CUDANear2FarMonitor:
         for n in FIELDS:
             setattr(self, f"{n}_dft", scatter(faces[n]))
         return faces
+
+
+class NumPyNear2FarMonitor:
+    """Host Huygens-box monitor: the reference ``NumPyNear2FarMonitor`` surface
+    (``opencl_fdtd_solver/monitors.py:186-380``) on any engine with ``Ex…Hz``.
+
+    Per step it accumulates the face-packed DFT on the host from the engine's
+    field reads with the reference arithmetic (``monitors.py:229-295``):
+    tangential samples co-located at face centres (2-point means of E, 4-point
+    means of H, clamped at the grid edge), E phase ``e^{jωt}·dt``, H phase
+    ``e^{jωt}·dt·e^{−jωdt/2}``, complex64 accumulators ``Ex_dft_f … Hz_dft_f`` in
+    the x0, x1, y0, y1, z0, z1 packing.  Each face is evaluated as array
+    operations instead of the per-sample loop, with the same operands in the
+    same order, so every accumulator rounds the same way.
+
+    The monitor declares ``host_regions`` (each face plane with the neighbouring
+    planes its means read), so on ``CUDAFDTD`` a step moves those slabs to the
+    host instead of six full volumes (``CUDAFDTD.host_window``).  On an engine
+    without windowed reads it reads full arrays, as the reference does.
+
+    ``get_farfield(s)`` runs the float64 surface sums on the device with the
+    OpenCL kernel's convention ``η·N⊥ − r̂×L`` (``dft_farfield.cl:617``).  The
+    reference's host ``get_farfield`` adds ``+ r̂×L`` (``monitors.py:378``), which
+    disagrees with its own kernel; the kernel convention is kept here.
+    """
+
+    def __init__(self, fdtd, center, size, freq):
+        self.fdtd = fdtd
+        self.freq = freq
+        self.omega = 2.0 * np.pi * freq
+        self.dl = fdtd.dl
+        cx, cy, cz = center
+        sx, sy, sz = size
+
+        def _idx(phys):
+            return int(round(phys / fdtd.dl))
+
+        self.ix0 = max(0, _idx(cx - sx / 2))
+        self.ix1 = min(fdtd.Nx - 1, _idx(cx + sx / 2))
+        self.iy0 = max(0, _idx(cy - sy / 2))
+        self.iy1 = min(fdtd.Ny - 1, _idx(cy + sy / 2))
+        self.iz0 = max(0, _idx(cz - sz / 2))
+        self.iz1 = min(fdtd.Nz - 1, _idx(cz + sz / 2))
+        if self.ix0 > self.ix1 or self.iy0 > self.iy1 or self.iz0 > self.iz1:
+            raise ValueError("Huygens box is empty after snapping to the grid")
+        self._faces = [("x", self.ix0, -1), ("x", self.ix1, +1), ("y", self.iy0, -1),
+                       ("y", self.iy1, +1), ("z", self.iz0, -1), ("z", self.iz1, +1)]
+        self._box = (self.ix0, self.ix1, self.iy0, self.iy1, self.iz0, self.iz1)
+        self.nxf = self.ix1 - self.ix0 + 1
+        self.nyf = self.iy1 - self.iy0 + 1
+        self.nzf = self.iz1 - self.iz0 + 1
+        self._face_counts = (self.nyf * self.nzf, self.nyf * self.nzf, self.nxf * self.nzf,
+                             self.nxf * self.nzf, self.nxf * self.nyf, self.nxf * self.nyf)
+        offs = [0]
+        for c in self._face_counts[:-1]:
+            offs.append(offs[-1] + c)
+        self._face_offsets = tuple(offs)
+        self.n_face_samples = int(sum(self._face_counts))
+        for n in FIELDS:
+            setattr(self, f"{n}_dft_f", np.zeros(self.n_face_samples, dtype=np.complex64))
+        # Volume placeholders of the reference (monitors.py:219-226); np.zeros
+        # reserves the pages lazily, so untouched volumes cost no memory.
+        shape = (fdtd.Nx, fdtd.Ny, fdtd.Nz)
+        for n in FIELDS:
+            setattr(self, f"{n}_dft", np.zeros(shape, dtype=np.complex64))
+        self._build_indices()
+        fdtd.add_monitor(self)
+
+    def _build_indices(self):
+        """Per axis: the face samples as a slice, their clamped ``+1`` neighbours
+        as a slice (an index array when the box touches the high edge, where the
+        reference clamps ``i+1`` to ``i``), and the mask of samples whose
+        neighbour differs from themselves."""
+        dims = (self.fdtd.Nx, self.fdtd.Ny, self.fdtd.Nz)
+        self._sel = []
+        for (lo, hi), n in zip(((self.ix0, self.ix1), (self.iy0, self.iy1),
+                                (self.iz0, self.iz1)), dims):
+            v = np.arange(lo, hi + 1)
+            v1 = np.where(v + 1 < n, v + 1, v)
+            nxt = slice(lo + 1, hi + 2) if hi + 1 < n else v1
+            self._sel.append((slice(lo, hi + 1), nxt, v1 != v))
+        # the same selections relative to the box corner, for the z-face slabs
+        # that __call__ copies out of the volume (k is the strided axis there)
+        self._rel = []
+        for (lo, hi), n in zip(((self.ix0, self.ix1), (self.iy0, self.iy1)), dims[:2]):
+            v = np.arange(lo, hi + 1)
+            v1 = np.where(v + 1 < n, v + 1, v)
+            nxt = slice(1, hi - lo + 2) if hi + 1 < n else v1 - lo
+            self._rel.append((slice(0, hi - lo + 1), nxt, min(hi + 2, n)))
+
+    def host_regions(self):
+        """Half-open boxes of every cell ``__call__`` reads: each face plane, the
+        plane below it (H means) and one extra row/column above the face (means)."""
+        nx, ny, nz = self.fdtd.Nx, self.fdtd.Ny, self.fdtd.Nz
+        ix0, ix1, iy0, iy1, iz0, iz1 = self._box
+        ih, jh, kh = min(ix1 + 2, nx), min(iy1 + 2, ny), min(iz1 + 2, nz)
+        regs = [((max(i - 1, 0), i + 1), (iy0, jh), (iz0, kh)) for i in (ix0, ix1)]
+        regs += [((ix0, ih), (max(j - 1, 0), j + 1), (iz0, kh)) for j in (iy0, iy1)]
+        regs += [((ix0, ih), (iy0, jh), (max(k - 1, 0), k + 1)) for k in (iz0, iz1)]
+        return regs
+
+    def __call__(self, fdtd):
+        phase_e = np.exp(1j * self.omega * fdtd.t) * fdtd.dt
+        phase_h = phase_e * np.exp(-0.5j * self.omega * fdtd.dt)
+        ph4 = phase_h * 0.25
+        Ex, Ey, Ez = np.asarray(fdtd.Ex), np.asarray(fdtd.Ey), np.asarray(fdtd.Ez)
+        Hx, Hy, Hz = np.asarray(fdtd.Hx), np.asarray(fdtd.Hy), np.asarray(fdtd.Hz)
+        (I, I1, okI), (J, J1, okJ), (K, K1, okK) = self._sel  # noqa: F841
+        o = self._face_offsets
+        c = self._face_counts
+
+        def at(plane, r, q):
+            # rows r and columns q of a 2-D plane view; slices stay views
+            if isinstance(r, slice) or isinstance(q, slice):
+                return plane[r, q]
+            return plane[np.ix_(r, q)]
+
+        def acc(arr, f, vals, ph):
+            arr[o[f]:o[f] + c[f]] += ph * vals.ravel()
+
+        rowJ, rowI, colK, colJ = okJ[:, None], okI[:, None], okK[None, :], okJ[None, :]
+        # x faces: samples (j, k), j outer.  Means: Ey over k, Ez over j, Hy over
+        # (i-1, j+1), Hz over (i-1, k+1), in the reference operand order.
+        for f, i in ((0, self.ix0), (1, self.ix1)):
+            il = i - 1 if i > 0 else i
+            a = at(Ey[i], J, K)
+            acc(self.Ey_dft_f, f, np.where(colK, 0.5 * (a + at(Ey[i], J, K1)), a), phase_e)
+            a = at(Ez[i], J, K)
+            acc(self.Ez_dft_f, f, np.where(rowJ, 0.5 * (a + at(Ez[i], J1, K)), a), phase_e)
+            acc(self.Hy_dft_f, f, at(Hy[i], J, K) + at(Hy[il], J, K) + at(Hy[i], J1, K)
+                + at(Hy[il], J1, K), ph4)
+            acc(self.Hz_dft_f, f, at(Hz[i], J, K) + at(Hz[il], J, K) + at(Hz[i], J, K1)
+                + at(Hz[il], J, K1), ph4)
+        # y faces: samples (i, k), i outer
+        for f, j in ((2, self.iy0), (3, self.iy1)):
+            jl = j - 1 if j > 0 else j
+            a = at(Ex[:, j], I, K)
+            acc(self.Ex_dft_f, f, np.where(colK, 0.5 * (a + at(Ex[:, j], I, K1)), a), phase_e)
+            a = at(Ez[:, j], I, K)
+            acc(self.Ez_dft_f, f, np.where(rowI, 0.5 * (a + at(Ez[:, j], I1, K)), a), phase_e)
+            acc(self.Hx_dft_f, f, at(Hx[:, j], I, K) + at(Hx[:, jl], I, K) + at(Hx[:, j], I1, K)
+                + at(Hx[:, jl], I1, K), ph4)
+            acc(self.Hz_dft_f, f, at(Hz[:, j], I, K) + at(Hz[:, jl], I, K) + at(Hz[:, j], I, K1)
+                + at(Hz[:, jl], I, K1), ph4)
+        # z faces: samples (i, j), i outer.  The planes are strided in memory, so
+        # each field's (i, j, kl..k) slab is copied once and indexed from the box corner.
+        (Ir, I1r, ie), (Jr, J1r, je) = self._rel
+        i0, j0 = self.ix0, self.iy0
+        for f, k in ((4, self.iz0), (5, self.iz1)):
+            kl = k - 1 if k > 0 else k
+
+            def slab(F):
+                s_ = np.ascontiguousarray(F[i0:ie, j0:je, kl:k + 1])
+                return s_[:, :, k - kl], s_[:, :, 0]
+
+            P, _ = slab(Ex)
+            a = at(P, Ir, Jr)
+            acc(self.Ex_dft_f, f, np.where(colJ, 0.5 * (a + at(P, Ir, J1r)), a), phase_e)
+            P, _ = slab(Ey)
+            a = at(P, Ir, Jr)
+            acc(self.Ey_dft_f, f, np.where(rowI, 0.5 * (a + at(P, I1r, Jr)), a), phase_e)
+            P, Q = slab(Hx)
+            acc(self.Hx_dft_f, f, at(P, Ir, Jr) + at(Q, Ir, Jr) + at(P, Ir, J1r)
+                + at(Q, Ir, J1r), ph4)
+            P, Q = slab(Hy)
+            acc(self.Hy_dft_f, f, at(P, Ir, Jr) + at(Q, Ir, Jr) + at(P, I1r, Jr)
+                + at(Q, I1r, Jr), ph4)
+
+    def get_farfields(self, obs_points) -> np.ndarray:
+        """Far E, H at many points (metres): ``(n_obs, 6)`` complex128."""
+        torch = _torch()
+        pts = _obs_array(obs_points, self.fdtd.dtype)
+        packed = np.stack([getattr(self, f"{n}_dft_f") for n in FIELDS])  # (6, n_face)
+        ri = np.stack([packed.real, packed.imag], axis=-1).astype(np.float64)[:, None]
+        with torch.cuda.stream(self.fdtd.queue):
+            acc = torch.from_numpy(np.ascontiguousarray(ri)).to(self.fdtd.device)
+        cbox = _box_struct(self._box, self._face_offsets, self.n_face_samples, 1)
+        return _device_farfields(self.fdtd, cbox, acc, 0, float(self.freq), pts)
+
+    def get_farfield(self, obs_point):
+        """Far E, H at one point (metres): ``(6,)`` complex128."""
+        return self.get_farfields([obs_point])[0]
 
 
 def _poynting_mag(ff) -> float:

@@ -94,3 +94,50 @@ def peak_err(a, b):
     den = float(np.max(np.abs(b)))
     num = float(np.max(np.abs(a - b)))
     return num / den if den > 0 else num
+
+
+class SyntheticFieldSequence:
+    """Engine stand-in that serves seeded random fields, one set per step.
+
+    It has the attributes a host monitor reads (``Nx, Ny, Nz, dl, dt, t``,
+    ``Ex … Hz``, ``add_monitor``), so the reference's ``NumPyNear2FarMonitor``
+    and this package's can be driven by identical inputs without a solver.
+    Step ``n`` draws from ``default_rng([seed, n])``.
+    """
+
+    FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+    def __init__(self, shape, dl, dt, seed, dtype=np.float32):
+        self.Nx, self.Ny, self.Nz = (int(v) for v in shape)
+        self.dl, self.dt, self.t = float(dl), float(dt), 0.0
+        self.dtype = np.dtype(dtype)
+        self.seed = int(seed)
+        self.step_num = 0
+        self._monitors = []
+        for n in self.FIELDS:
+            setattr(self, n, np.zeros((self.Nx, self.Ny, self.Nz), self.dtype))
+
+    def add_monitor(self, mon):
+        self._monitors.append(mon)
+        return mon
+
+    def step(self):
+        rng = np.random.default_rng([self.seed, self.step_num])
+        for n in self.FIELDS:
+            setattr(self, n, rng.standard_normal((self.Nx, self.Ny, self.Nz)).astype(self.dtype))
+        self.step_num += 1
+        self.t += self.dt
+        for mon in self._monitors:
+            mon(self)
+
+
+# Host-monitor fixture cases: (tag, shape, dl, dt, seed, center, size, freq, steps).
+# "inner" keeps the box away from the grid edges; "edge" snaps it to the whole
+# grid, so every clamp of the co-location means (i+1, j+1, k+1 at the high edge,
+# i-1 at index 0) is exercised.
+HOST_MONITOR_CASES = (
+    ("inner", (12, 14, 16), 2e-3, 3.1e-12, 11, (12e-3, 14e-3, 16e-3), (10e-3, 12e-3, 14e-3),
+     5e9, 6),
+    ("edge", (9, 10, 11), 1e-3, 1.7e-12, 12, (4.5e-3, 5e-3, 5.5e-3), (20e-3, 20e-3, 20e-3),
+     8e9, 5),
+)

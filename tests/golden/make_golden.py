@@ -14,6 +14,9 @@ Outputs:
 * ``ocl_farfield.npz`` — the reference's committed OpenCL far-field arrays
   (``ocl_eh_plus_{z,x}``, ``ocl_S_db``, ``angles_deg``) for ``vacuum_farfield`` and
   ``dielectric_sphere_farfield`` (case: ``tests/meep_validation/cases.py:24-83``).
+* ``host_monitor.npz`` — face-packed DFT arrays ``*_dft_f`` of the reference's
+  ``NumPyNear2FarMonitor`` (``opencl_fdtd_solver/monitors.py:186-295``) driven by
+  the seeded field sequences of ``tests/cases.py`` (``HOST_MONITOR_CASES``).
 * ``numpy_ref.npz``    — fields produced by importing the reference's own
   ``NumPyFDTD`` / ``NumPyFDTD_FaceCPML`` (with a stub ``pyopencl`` module, which the
   reference imports at top level but only uses at call time) on small cases, plus
@@ -156,11 +159,34 @@ def numpy_cases(ref):
     return out
 
 
+def host_monitor_cases(ref):
+    sys.path.insert(0, str(HERE.parents[1]))
+    from tests.cases import HOST_MONITOR_CASES, SyntheticFieldSequence
+
+    out = {}
+    for tag, shape, dl, dt, seed, center, size, freq, steps in HOST_MONITOR_CASES:
+        seq = SyntheticFieldSequence(shape, dl, dt, seed)
+        mon = ref.NumPyNear2FarMonitor(seq, center, size, freq)
+        for _ in range(steps):
+            seq.step()
+        out[f"{tag}_box"] = np.array(mon._box)
+        for n in SyntheticFieldSequence.FIELDS:
+            out[f"{tag}_{n}_dft_f"] = getattr(mon, f"{n}_dft_f").copy()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=("host_monitor",), default=None,
+                    help="write just this fixture")
     args = ap.parse_args(argv)
     root = Path(args.reference)
+    if args.only == "host_monitor":
+        ref = import_reference(root)
+        np.savez_compressed(HERE / "host_monitor.npz", **host_monitor_cases(ref))
+        print("wrote host_monitor.npz")
+        return
     base = root / "tests/meep_validation/baselines"
     planes = {}
     for case in ("vacuum_sheet", "dielectric_block"):
@@ -175,6 +201,7 @@ def main(argv=None):
     warnings.simplefilter("ignore", DeprecationWarning)
     ref = import_reference(root)
     np.savez_compressed(HERE / "numpy_ref.npz", **numpy_cases(ref))
+    np.savez_compressed(HERE / "host_monitor.npz", **host_monitor_cases(ref))
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 

@@ -44,7 +44,8 @@ def test_ctypes_structs_match_c_header(tmp_path):
     structs = {"fdtd_grid": capi.Grid, "fdtd_fields": capi.Fields, "fdtd_cpml": capi.Cpml,
                "fdtd_source": capi.Source, "fdtd_plane_dft": capi.PlaneDft, "fdtd_box": capi.Box,
                "fdtd_adjoint_fields": capi.AdjointFields, "fdtd_adjoint_seed": capi.AdjointSeed,
-               "fdtd_grad_box": capi.GradBox, "fdtd_n2f_face": capi.N2FFace}
+               "fdtd_grad_box": capi.GradBox, "fdtd_n2f_face": capi.N2FFace,
+               "fdtd_region": capi.Region}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fdtd_b200.h"',
              'int main(void) {']
     for cname, py in structs.items():
@@ -82,6 +83,32 @@ def test_invalid_arguments_return_status_without_launch():
     g = capi.Grid(nx=4, ny=4, nz=4, npml=0, dtype=0)
     assert capi.call("fdtd_update_H", g, f, c, None) == capi.FDTD_ERR_INVALID  # NULL fields
     assert capi.call("fdtd_farfield", None, None, 0, 1.0, 1.0, 1.0, None, 1, None, None,
+                     None) == capi.FDTD_ERR_INVALID
+
+
+def test_read_regions_validates_boxes_without_launch():
+    regs = (capi.Region * 2)()
+    regs[0].lo[:] = (0, 0, 0)
+    regs[0].hi[:] = (4, 5, 0)          # empty along k
+    regs[1].lo[:] = (2, 2, 2)
+    regs[1].hi[:] = (2, 5, 6)          # empty along i
+    # all boxes empty: nothing to copy, so no buffers are needed
+    assert capi.call("fdtd_read_regions", None, 0, 4, 5, 6, regs, 2, None, None, None) == 0
+    regs[1].lo[0] = 3                  # lo > hi
+    assert capi.call("fdtd_read_regions", None, 0, 4, 5, 6, regs, 2, None, None,
+                     None) == capi.FDTD_ERR_INVALID
+    assert "region 1 axis 0" in capi.last_error()
+    regs[1].lo[0], regs[1].hi[2] = 2, 7   # hi beyond Nz
+    assert capi.call("fdtd_read_regions", None, 0, 4, 5, 6, regs, 2, None, None,
+                     None) == capi.FDTD_ERR_INVALID
+    regs[1].hi[:] = (3, 5, 6)          # valid, non-empty: buffers are required
+    assert capi.call("fdtd_read_regions", None, 0, 4, 5, 6, regs, 2, None, None,
+                     None) == capi.FDTD_ERR_INVALID
+    assert "NULL" in capi.last_error()
+    many = (capi.Region * (capi.FDTD_MAX_REGIONS + 1))()
+    assert capi.call("fdtd_read_regions", None, 0, 4, 5, 6, many, capi.FDTD_MAX_REGIONS + 1,
+                     None, None, None) == capi.FDTD_ERR_INVALID
+    assert capi.call("fdtd_read_regions", None, 3, 4, 5, 6, regs, 1, None, None,
                      None) == capi.FDTD_ERR_INVALID
 
 
