@@ -516,16 +516,18 @@ def test_launch_counter_and_step_profile(cuda):
     assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
 
 
-def test_medium_config_sphere_box_farfield(cuda):
-    """The medium configuration, shortened to 200 steps: 256³ FP32, npml 12, εr = 4
-    sphere of radius 40 cells, rim-tapered Jx sheet at z = npml + 8 trimmed out of
-    the PML, Gaussian-modulated sine, a closed 6-face DFT box (half-width 44 cells)
-    at 8 frequencies, far field on a 181 (θ) x 91 (φ) grid at R = 1 m.  Fields and
-    box DFTs against the C oracle; far fields direct and through the tensor-core
-    contraction against the oracle's float64 transform."""
+@pytest.mark.parametrize("steps", [200, 2000], ids=["200_steps", "full_2000_steps"])
+def test_medium_config_sphere_box_farfield(cuda, steps):
+    """The medium configuration: 256³ FP32, npml 12, εr = 4 sphere of radius 40
+    cells, rim-tapered Jx sheet at z = npml + 8 trimmed out of the PML,
+    Gaussian-modulated sine, a closed 6-face DFT box (half-width 44 cells) at 8
+    frequencies, far field on a 181 (θ) x 91 (φ) grid at R = 1 m; 200 steps and
+    the configuration's full 2000.  Fields and box DFTs against the C oracle; far
+    fields direct and through the tensor-core contraction against the oracle's
+    float64 transform."""
     from oracle.dft_oracle import OracleNear2FarMonitor
 
-    n, npml, dl, steps = 256, 12, 1e-3, 200
+    n, npml, dl = 256, 12, 1e-3
     shape = (n, n, n)
     eps = sphere_eps(shape, n // 2, 40, 4.0)
     freqs = np.linspace(20e9, 40e9, 8)
