@@ -80,36 +80,70 @@ class _PhaseTable:
     """Device table of the per-step phases ``[chunk][nfreq][4]`` (E re, E im, H re, H im).
 
     The first call uses ``e^{jωt}·dt``; later calls multiply by ``e^{jωdt}``
-    (reference ``monitors.py:571-577``), computed ahead a chunk at a time.
+    (reference ``monitors.py:571-577``), computed ahead a chunk at a time.  Each
+    chunk goes up through one of two pinned host buffers with an asynchronous
+    copy on the engine's stream into one of two device tables, so refilling
+    never waits for the device to catch up with the host; a pinned buffer is
+    refilled only after its previous copy completed (an event), and a device
+    table is overwritten in stream order after the steps that read it.  Without
+    a stream the table stays on the host (the phase sequence alone).
     """
 
-    def __init__(self, freqs, dt, device):
+    def __init__(self, freqs, dt, device, stream=None):
         self.omega = 2.0 * np.pi * np.asarray(freqs, dtype=np.float64)
         self.dt = float(dt)
         self.dphase = np.exp(1j * self.omega * self.dt)
         self.half = np.exp(-0.5j * self.omega * self.dt)
         self.device = device
+        self.stream = stream
         self.phase = None  # host value of the most recent step (complex128 [nfreq])
-        self._host = None
+        self._pin = self._dev_tabs = self._done = None
         self._dev = None
+        self._slot = 1
         self._cursor = 0
 
     def _fill(self, first):
+        torch = _torch()
         nf = self.omega.size
-        host = np.empty((_PHASE_CHUNK, nf, 4), np.float64)
+        if self.stream is None:  # host-only table (no device upload)
+            self._seq = self._sequence(first)
+            self._dev = torch.zeros(1)
+            self._cursor = 0
+            return
+        if self._pin is None:
+            shape = (_PHASE_CHUNK, nf, 4)
+            self._pin = [torch.empty(shape, dtype=torch.float64, pin_memory=True)
+                         for _ in range(2)]
+            with torch.cuda.stream(self.stream):
+                self._dev_tabs = [torch.empty(shape, dtype=torch.float64, device=self.device)
+                                  for _ in range(2)]
+            self._done = [None, None]
+        seq = self._sequence(first)
+        ph = seq * self.half
+        self._slot ^= 1
+        b = self._slot
+        if self._done[b] is not None:
+            self._done[b].synchronize()  # the copy from this pinned buffer has landed
+        host = self._pin[b].numpy()
+        host[:, :, 0], host[:, :, 1] = seq.real, seq.imag
+        host[:, :, 2], host[:, :, 3] = ph.real, ph.imag
+        self._seq = seq
+        with torch.cuda.stream(self.stream):
+            self._dev_tabs[b].copy_(self._pin[b], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        self._done[b] = ev
+        self._dev = self._dev_tabs[b]
+        self._cursor = 0
+
+    def _sequence(self, first):
         p = first
-        seq = np.empty((_PHASE_CHUNK, nf), np.complex128)
+        seq = np.empty((_PHASE_CHUNK, self.omega.size), np.complex128)
         for s in range(_PHASE_CHUNK):
             if s > 0:
                 p = p * self.dphase
             seq[s] = p
-        ph = seq * self.half
-        host[:, :, 0], host[:, :, 1] = seq.real, seq.imag
-        host[:, :, 2], host[:, :, 3] = ph.real, ph.imag
-        self._seq = seq
-        torch = _torch()
-        self._dev = torch.from_numpy(host).to(self.device)
-        self._cursor = 0
+        return seq
 
     def next_ptr(self, t):
         """Advance one step (monitor time ``t``) and return the device pointer of its phases."""
@@ -156,7 +190,7 @@ class CUDAPlaneDFTMonitor:
         with torch.cuda.stream(fdtd.queue):
             self.acc = torch.zeros((len(self.components), self.freqs.size, *dims, 2),
                                    dtype=torch.float64, device=fdtd.device)
-        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device)
+        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device, fdtd.queue)
         n_planes = sum(1 for m in fdtd._monitors if isinstance(m, CUDAPlaneDFTMonitor))
         if n_planes >= capi.FDTD_MAX_PLANES:
             raise ValueError(f"at most {capi.FDTD_MAX_PLANES} plane DFT monitors per engine")
@@ -235,7 +269,7 @@ class CUDANear2FarMonitor:
         with torch.cuda.stream(fdtd.queue):
             self.acc = torch.zeros((6, self.freqs.size, self.n_face_samples, 2),
                                    dtype=torch.float64, device=fdtd.device)
-        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device)
+        self._phases = _PhaseTable(self.freqs, fdtd.dt, fdtd.device, fdtd.queue)
         self._dft_snap = None
         self.Ex_dft = self.Ey_dft = self.Ez_dft = None
         self.Hx_dft = self.Hy_dft = self.Hz_dft = None
