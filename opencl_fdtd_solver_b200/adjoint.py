@@ -7,23 +7,28 @@ one on top of :class:`CUDAFDTD` without changing the forward path:
   box), runs ``n_steps`` from rest with the engine's registered sources, accumulates
   a plane DFT on the objective plane (the same kernel and phase recurrence as
   :class:`CUDAPlaneDFTMonitor`, reference ``monitors.py:571-584``), evaluates
-  ``J = fn(D)`` on the patch and keeps a checkpoint of the full state every
-  ``checkpoint_every`` steps (fields and ψ stripes: ``CUDAFDTD.save_state``).
+  ``J = fn(D)`` on the patch.  The sweep needs the forward ``E`` over the design's
+  edge box at every step (``fdtd_capture_box``).  When all ``n_steps + 1`` boxes
+  fit the capture budget (a quarter of the free device memory by default; 5.8 GB
+  for a 96×96×16 design over 3000 steps), the forward pass captures them all;
+  otherwise it keeps a checkpoint of the full state every ``checkpoint_every``
+  steps (fields and ψ stripes: ``CUDAFDTD.save_state``) for replay.
 * ``backward()`` runs the adjoint sweep: ``∂J/∂D`` (by torch autograd through ``fn``)
   seeds ``Ē`` on the patch each step (``fdtd_adjoint_seed_add`` / the seed of
-  ``fdtd_adjoint_step``); segments are replayed from their checkpoints, newest
-  first, with ``E`` captured over the design's edge box each step
-  (``fdtd_capture_box``), and the transposed step runs backwards through the segment
-  (``fdtd_adjoint_step``) on a second stream, concurrently with the replay of the
-  next-older segment (two capture buffers, ordered by events), accumulating ``Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce``
-  on the edge box in float64.  The host chain rule through ``ce = dt/(ε0·ε_edge)``
-  and the two-cell edge average (reference ``materials.py:28-56``) gives
-  ``∂J/∂εr`` per design cell.
+  ``fdtd_adjoint_step``) and the transposed step runs backwards in time
+  (``fdtd_adjoint_step``), accumulating ``Σ_n Ē^{n+1}·(E^{n+1} − E^n) = ce·∂J/∂ce``
+  on the edge box in float64.  With checkpoints, segments are replayed newest
+  first with ``E`` captured each step, and the sweep through a segment runs on a
+  second stream, concurrently with the replay of the next-older segment (two
+  capture buffers, ordered by events).  The host chain rule through
+  ``ce = dt/(ε0·ε_edge)`` and the two-cell edge average (reference
+  ``materials.py:28-56``) gives ``∂J/∂εr`` per design cell.
 * :class:`EpsilonObjective` wraps the pair as a ``torch.autograd.Function``.
 
 The gradient is exact for the discrete scheme (lossless grids: ``set_epsilon``
-without σ); its cost is one forward solve, one replayed forward solve and one
-adjoint sweep.
+without σ) and the same bit for bit in both capture modes; its cost is one
+forward solve and one adjoint sweep, plus one replayed forward solve in the
+checkpoint mode.
 """
 
 from __future__ import annotations
@@ -140,13 +145,18 @@ class EpsilonAdjoint:
     n_steps          : time steps per solve (from rest at t = 0)
     objective        : :class:`DFTObjective`
     eps_background   : cell-centred ``εr`` outside the design box (default 1)
-    checkpoint_every : steps per replayed segment (K)
+    checkpoint_every : steps per replayed segment (K) in the checkpoint mode
+    capture          : ``"auto"`` (default): keep the forward ``E`` over the edge box
+                       for every step when that fits ``capture_budget`` bytes, else
+                       checkpoint and replay; ``"all"`` or ``"replay"`` force a mode
+    capture_budget   : bytes the ``"auto"`` mode may hold (default: a quarter of the
+                       device memory free at the forward call)
 
     The engine's own monitors are detached while this object steps it.
     """
 
     def __init__(self, fdtd, design, n_steps, objective, *, eps_background=None,
-                 checkpoint_every=100):
+                 checkpoint_every=100, capture="auto", capture_budget=None):
         if not isinstance(fdtd, CUDAFDTD):
             raise TypeError("EpsilonAdjoint needs a CUDAFDTD engine")
         self.fdtd = fdtd
@@ -161,6 +171,10 @@ class EpsilonAdjoint:
         self.K = int(checkpoint_every)
         if self.K < 1:
             raise ValueError("checkpoint_every must be >= 1")
+        if capture not in ("auto", "all", "replay"):
+            raise ValueError(f"capture must be 'auto', 'all' or 'replay', got {capture!r}")
+        self.capture = capture
+        self.capture_budget = None if capture_budget is None else int(capture_budget)
         if not isinstance(objective, DFTObjective):
             raise TypeError("objective must be a DFTObjective")
         self.objective = objective
@@ -182,6 +196,8 @@ class EpsilonAdjoint:
         self.box = tuple((max(0, lo - 1), hi) for lo, hi in self.design)
         self.box_shape = tuple(hi - lo for lo, hi in self.box)
         self._ckpts = None
+        self._cap_all = None   # (n_steps + 1, 3, box) forward E, in the capture-all mode
+        self._captured = False
         self._seed = None
         self.J = None
         self.D = None
@@ -203,18 +219,36 @@ class EpsilonAdjoint:
         self._eps = self._eps_full(eps_design)
         fd.set_epsilon(self._eps)
         fd.reset_state()
+        capture_all = self._capture_all()
         saved = fd._monitors
         fd._monitors = []
         ckpts = []
         try:
             mon = CUDAPlaneDFTMonitor(fd, o.axis, o.index, o.freqs, o.components)
             self._t_first = fd.t + fd.dt
-            for n in range(self.n_steps):
-                if n % self.K == 0:
-                    ckpts.append(fd.save_state())
-                fd.step()
+            if capture_all:
+                grid, st = fd._grid, fd.queue.cuda_stream
+                lo = (ctypes.c_int32 * 3)(*[b[0] for b in self.box])
+                hi = (ctypes.c_int32 * 3)(*[b[1] for b in self.box])
+                cap0 = self._cap_all.data_ptr()
+                slot = self._cap_all[0].numel() * self._cap_all.element_size()
+
+                def grab(m):
+                    Ep = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in fd._E])
+                    capi.run("fdtd_capture_box", grid, Ep, lo, hi, cap0 + m * slot, st)
+
+                grab(0)
+                for n in range(self.n_steps):
+                    fd.step()
+                    grab(n + 1)
+            else:
+                for n in range(self.n_steps):
+                    if n % self.K == 0:
+                        ckpts.append(fd.save_state())
+                    fd.step()
         finally:
             fd._monitors = saved
+        self._captured = capture_all
         self._ckpts = ckpts
         (a0, a1), (b0, b1) = o.patch
         D = torch.view_as_complex(mon.acc)[:, :, a0:a1, b0:b1].detach().clone()
@@ -226,6 +260,30 @@ class EpsilonAdjoint:
         self.D = D
         self.J = float(J.detach())
         return self.J
+
+    def _capture_all(self):
+        """Whether this forward keeps E over the edge box for every step; allocates
+        (or reuses) the buffer when it does."""
+        fd = self.fdtd
+        shape = (self.n_steps + 1, 3, *self.box_shape)
+        nbytes = int(np.prod(shape)) * np.dtype(fd.dtype).itemsize
+        if self.capture == "replay":
+            self._cap_all = None
+            return False
+        if self.capture == "auto" and (self._cap_all is None or
+                                       tuple(self._cap_all.shape) != shape):
+            budget = self.capture_budget
+            if budget is None:
+                free, _ = torch.cuda.mem_get_info(fd.device)
+                budget = free // 4
+            if nbytes > budget:
+                self._cap_all = None
+                return False
+        if self._cap_all is None or tuple(self._cap_all.shape) != shape:
+            self._cap_all = None
+            with torch.cuda.stream(fd.queue):
+                self._cap_all = torch.empty(shape, dtype=fd._tdt, device=fd.device)
+        return True
 
     # ---------------------------------------------------------------- backward
     def _adjoint_buffers(self):
@@ -257,6 +315,8 @@ class EpsilonAdjoint:
         """``grad_output · ∂J/∂εr`` over the design box (float64 NumPy array)."""
         if self._ckpts is None:
             raise RuntimeError("call forward() before backward()")
+        if self._captured:
+            return self._backward_captured(grad_output)
         fd = self.fdtd
         o = self.objective
         if fd.lossy:
@@ -264,24 +324,12 @@ class EpsilonAdjoint:
         st = fd.queue.cuda_stream
         N, K = self.n_steps, self.K
         nseg = len(self._ckpts)
+        Eb, Hb, PE, PH, fields, ph_dev, G, sd, gb = self._sweep_setup()
         with torch.cuda.stream(fd.queue):
-            Eb, Hb, PE, PH, fields = self._adjoint_buffers()
-            phases = _phase_sequence(o.freqs, fd.dt, N, self._t_first)
-            ph_dev = torch.from_numpy(np.ascontiguousarray(
-                np.stack([phases.real, phases.imag], -1))).to(fd.device)
-            G = torch.zeros((3, *self.box_shape), dtype=torch.float64, device=fd.device)
             # two capture buffers: segment s is swept while segment s-1 is replayed
             cap = torch.empty((2, K + 1, 3, *self.box_shape), dtype=fd._tdt, device=fd.device)
-        (a0, a1), (b0, b1) = o.patch
-        sd = capi.AdjointSeed(axis=o.axis, index=o.index, a0=a0, a1=a1, b0=b0, b1=b1,
-                              comp_mask=o.comp_mask, nfreq=o.freqs.size,
-                              seed=self._seed.data_ptr(), phase=0)
         ph_stride = o.freqs.size * 2 * 8
         ph0 = ph_dev.data_ptr()
-        gb = capi.GradBox()
-        for a in range(3):
-            gb.lo[a], gb.hi[a] = self.box[a]
-        gb.g = G.data_ptr()
         lo = (ctypes.c_int32 * 3)(*[b[0] for b in self.box])
         hi = (ctypes.c_int32 * 3)(*[b[1] for b in self.box])
         slot = cap[0, 0].numel() * cap.element_size()
@@ -353,6 +401,58 @@ class EpsilonAdjoint:
             fd._monitors = saved
             adj.synchronize()
             fd.queue.synchronize()
+        self._adjoint_state = (Eb, Hb)
+        g_edges = G.cpu().numpy()
+        return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)
+
+    def _sweep_setup(self):
+        fd = self.fdtd
+        o = self.objective
+        N = self.n_steps
+        with torch.cuda.stream(fd.queue):
+            Eb, Hb, PE, PH, fields = self._adjoint_buffers()
+            phases = _phase_sequence(o.freqs, fd.dt, N, self._t_first)
+            ph_dev = torch.from_numpy(np.ascontiguousarray(
+                np.stack([phases.real, phases.imag], -1))).to(fd.device)
+            G = torch.zeros((3, *self.box_shape), dtype=torch.float64, device=fd.device)
+        (a0, a1), (b0, b1) = o.patch
+        sd = capi.AdjointSeed(axis=o.axis, index=o.index, a0=a0, a1=a1, b0=b0, b1=b1,
+                              comp_mask=o.comp_mask, nfreq=o.freqs.size,
+                              seed=self._seed.data_ptr(), phase=0)
+        gb = capi.GradBox()
+        for a in range(3):
+            gb.lo[a], gb.hi[a] = self.box[a]
+        gb.g = G.data_ptr()
+        return Eb, Hb, PE, PH, fields, ph_dev, G, sd, gb
+
+    def _backward_captured(self, grad_output):
+        """The sweep over E captured by the forward pass: no replay."""
+        fd = self.fdtd
+        if fd.lossy:
+            raise NotImplementedError("the adjoint gradient needs a lossless grid")
+        N = self.n_steps
+        st = fd.queue.cuda_stream
+        Eb, Hb, PE, PH, fields, ph_dev, G, sd, gb = self._sweep_setup()
+        ph_stride = self.objective.freqs.size * 2 * 8
+        ph0 = ph_dev.data_ptr()
+        cap0 = self._cap_all.data_ptr()
+        slot = self._cap_all[0].numel() * self._cap_all.element_size()
+        grid, cpml = fd._grid, fd._cpml_base
+        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb])
+        sd.phase = ph0 + (N - 1) * ph_stride
+        capi.run("fdtd_adjoint_seed_add", grid, Ebp, sd, st)
+        par = 0
+        for n in range(N - 1, -1, -1):
+            gb.e_next = cap0 + (n + 1) * slot
+            gb.e_prev = cap0 + n * slot
+            if n >= 1:
+                sd.phase = ph0 + (n - 1) * ph_stride
+                seed_arg = ctypes.byref(sd)
+            else:
+                seed_arg = None
+            capi.run("fdtd_adjoint_step", grid, fields[par], cpml, gb, seed_arg, st)
+            par ^= 1
+        fd.queue.synchronize()
         self._adjoint_state = (Eb, Hb)
         g_edges = G.cpu().numpy()
         return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)

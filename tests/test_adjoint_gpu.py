@@ -7,8 +7,8 @@ Checks, in order of strength:
 * against torch autograd through the FP64 transcription of the reference NumPy
   engine (``oracle/torch_fdtd.py``) on a 48³ grid;
 * against central finite differences (h = 1e-3) of the CUDA forward solve;
-* checkpoint spacing does not change the result; the autograd wrapper returns
-  the same gradient; lossy grids are refused.
+* checkpoint spacing and the capture mode do not change the result; the
+  autograd wrapper returns the same gradient; lossy grids are refused.
 """
 
 from __future__ import annotations
@@ -49,13 +49,13 @@ def _full(shape, design, eps_d):
     return eps
 
 
-def _cuda_adjoint(case, dtype, n_steps, K):
+def _cuda_adjoint(case, dtype, n_steps, K, **kw):
     z, i0, i1, j0, j1 = case["src"]
     fd = CUDAFDTD(case["shape"], DL, npml=case["npml"], dtype=dtype)
     fd.add_source(lambda f: f.add_source_Jx(z, _drive(f.t), i0, i1, j0, j1, rim_taper=True))
     o = case["obj"]
     obj = DFTObjective(o["axis"], o["index"], o["patch"], o["freqs"], o["components"])
-    return EpsilonAdjoint(fd, case["design"], n_steps, obj, checkpoint_every=K)
+    return EpsilonAdjoint(fd, case["design"], n_steps, obj, checkpoint_every=K, **kw)
 
 
 def _oracle(case, dtype, n_steps, eps_d):
@@ -81,13 +81,33 @@ def test_cuda_adjoint_matches_oracle(dtype, tol):
 
 
 def test_checkpoint_spacing_does_not_change_gradient():
+    """Replay from checkpoints every K steps (K = 1000, 7, 1) and the forward
+    capture of every step give the same gradient bit for bit."""
     eps_d = _eps_design(SMALL["design"], 2)
     g = []
     for K in (1000, 7, 1):
-        adj = _cuda_adjoint(SMALL, np.float32, 90, K)
+        adj = _cuda_adjoint(SMALL, np.float32, 90, K, capture="replay")
         g.append(adj.value_and_grad(eps_d)[1])
-    np.testing.assert_array_equal(g[0], g[1])
-    np.testing.assert_array_equal(g[0], g[2])
+        assert not adj._captured and adj._cap_all is None
+    adj = _cuda_adjoint(SMALL, np.float32, 90, 7, capture="all")
+    g.append(adj.value_and_grad(eps_d)[1])
+    assert adj._captured
+    for other in g[1:]:
+        np.testing.assert_array_equal(g[0], other)
+
+
+def test_capture_mode_follows_the_budget():
+    eps_d = _eps_design(SMALL["design"], 4)
+    roomy = _cuda_adjoint(SMALL, np.float64, 60, 10)
+    J0, g0 = roomy.value_and_grad(eps_d)
+    assert roomy._captured  # a few MB: within a quarter of free memory
+    tight = _cuda_adjoint(SMALL, np.float64, 60, 10, capture_budget=0)
+    J1, g1 = tight.value_and_grad(eps_d)
+    assert not tight._captured and tight._cap_all is None
+    assert J0 == J1
+    np.testing.assert_array_equal(g0, g1)
+    with pytest.raises(ValueError):
+        _cuda_adjoint(SMALL, np.float64, 60, 10, capture="sometimes")
 
 
 def test_autograd_function_returns_adjoint_gradient():
