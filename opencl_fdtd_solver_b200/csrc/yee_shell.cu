@@ -18,7 +18,7 @@
 //   A: i outside [lo_x, hi_x)                      all (j, k)
 //   B: i inside,  j outside [lo_y, hi_y)           all k
 //   C: i inside,  j inside,  k outside [lo_z, hi_z)
-// decoded with 32-bit divisions (consecutive threads take consecutive k).
+// decoded with multiply-high divisions (consecutive threads take consecutive k).
 #include <cuda_runtime.h>
 
 #include "launch_count.cuh"
@@ -26,42 +26,66 @@
 
 namespace fdtd {
 
-// Host-precomputed sizes of the three groups.
+// Unsigned 32-bit division by a divisor fixed at launch: a multiply-high and a
+// shift in place of the runtime division sequence (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, round-up
+// variant): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (umulhi(m, n) + n) >> l for every 32-bit n, the sum taken in 64 bits.
+struct FastDiv {
+    unsigned d, m, l;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d ? d : 1u;  // empty groups never divide
+    f.l = 0;
+    while ((1ull << f.l) < f.d) ++f.l;
+    f.m = (unsigned)(((1ull << 32) * ((1ull << f.l) - f.d)) / f.d + 1ull);
+    return f;
+}
+
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) {
+    return (unsigned)(((unsigned long long)__umulhi(n, f.m) + n) >> f.l);
+}
+
+// Host-precomputed sizes of the three groups and their divisors.
 struct ShellPlan {
     ShellBox b;
     int nax, nay, bx, by, cpr;  // slab planes in x, slab rows in y, box extents, C cells/row
     unsigned nA, nB, nC;        // cells per group
+    FastDiv d_plane, d_nz, d_slab, d_cpr, d_by;  // ny*nz, nz, nay*nz, cpr, by
 };
 
 __device__ __forceinline__ bool shell_cell(unsigned t, int nx, int ny, int nz,
                                            const ShellPlan &s, int &i, int &j, int &k) {
     (void)nx;
+    (void)ny;
     if (t < s.nA) {
-        const unsigned plane = (unsigned)ny * (unsigned)nz;
-        const int q = (int)(t / plane);
-        const unsigned rem = t - (unsigned)q * plane;
-        i = q < s.b.lo[0] ? q : s.b.hi[0] + (q - s.b.lo[0]);
-        j = (int)(rem / (unsigned)nz);
-        k = (int)(rem - (unsigned)j * (unsigned)nz);
+        const unsigned q = fdiv(t, s.d_plane);
+        const unsigned rem = t - q * s.d_plane.d;
+        i = (int)q < s.b.lo[0] ? (int)q : s.b.hi[0] + ((int)q - s.b.lo[0]);
+        const unsigned jj = fdiv(rem, s.d_nz);
+        j = (int)jj;
+        k = (int)(rem - jj * (unsigned)nz);
         return true;
     }
     t -= s.nA;
     if (t < s.nB) {
-        const unsigned slab = (unsigned)s.nay * (unsigned)nz;
-        const int q = (int)(t / slab);
-        const unsigned rem = t - (unsigned)q * slab;
-        i = s.b.lo[0] + q;
-        const int r = (int)(rem / (unsigned)nz);
-        j = r < s.b.lo[1] ? r : s.b.hi[1] + (r - s.b.lo[1]);
-        k = (int)(rem - (unsigned)r * (unsigned)nz);
+        const unsigned q = fdiv(t, s.d_slab);
+        const unsigned rem = t - q * s.d_slab.d;
+        i = s.b.lo[0] + (int)q;
+        const unsigned r = fdiv(rem, s.d_nz);
+        j = (int)r < s.b.lo[1] ? (int)r : s.b.hi[1] + ((int)r - s.b.lo[1]);
+        k = (int)(rem - r * (unsigned)nz);
         return true;
     }
     t -= s.nB;
     if (t < s.nC) {
-        const int row = (int)(t / (unsigned)s.cpr);
-        const int c = (int)(t - (unsigned)row * (unsigned)s.cpr);
-        i = s.b.lo[0] + row / s.by;
-        j = s.b.lo[1] + row % s.by;
+        const unsigned row = fdiv(t, s.d_cpr);
+        const int c = (int)(t - row * (unsigned)s.cpr);
+        const unsigned bi = fdiv(row, s.d_by);
+        i = s.b.lo[0] + (int)bi;
+        j = s.b.lo[1] + (int)(row - bi * (unsigned)s.by);
         k = c < s.b.lo[2] ? c : s.b.hi[2] + (c - s.b.lo[2]);
         return true;
     }
@@ -79,6 +103,11 @@ ShellPlan make_plan(int nx, int ny, int nz, const ShellBox &b) {
     s.nA = (unsigned)((int64_t)s.nax * ny * nz);
     s.nB = (unsigned)((int64_t)s.bx * s.nay * nz);
     s.nC = (unsigned)((int64_t)s.bx * s.by * s.cpr);
+    s.d_plane = make_fastdiv((unsigned)ny * (unsigned)nz);
+    s.d_nz = make_fastdiv((unsigned)nz);
+    s.d_slab = make_fastdiv((unsigned)s.nay * (unsigned)nz);
+    s.d_cpr = make_fastdiv((unsigned)(s.cpr > 0 ? s.cpr : 0));
+    s.d_by = make_fastdiv((unsigned)(s.by > 0 ? s.by : 0));
     return s;
 }
 
