@@ -54,30 +54,39 @@ constexpr double C0 = 299792458.0;
 
 template <int MODE>
 struct Cfg;
+// A stage holds KR real K values: NCH 16-byte K chunks per operand row, MPS
+// MMAs of two chunks each (K = 16 BF16 or 8 TF32 per MMA).  Wider stages
+// amortise the per-stage barrier round trips over more MMAs.
 template <>
 struct Cfg<FDTD_N2F_BF16X3> {
-    static constexpr int KR = 16;                 // real K per stage (one MMA K)
-    static constexpr int PS = 8;                  // complex samples p per stage
+    static constexpr int KR = 32;                 // real K per stage
+    static constexpr int PS = KR / 2;             // complex samples p per stage
+    static constexpr int NCH = KR / 8;            // 16-byte chunks per row
+    static constexpr int MPS = NCH / 2;           // MMA K groups per stage
     static constexpr int A_BYTES = BM * KR * 2;   // one of hi / lo
     static constexpr int B_BYTES = BN * KR * 2;   // one of hi / lo
     static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int B_COPY = 2 * B_BYTES;
-    static constexpr int NST = 8;  // 192 KB of stages: one CTA per SM
+    static constexpr int NST = (192 * 1024) / STAGE;  // 192 KB of stages: one CTA per SM
     static constexpr uint32_t IDESC =
         (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 };
 template <>
 struct Cfg<FDTD_N2F_TF32> {
-    static constexpr int KR = 8;
-    static constexpr int PS = 4;
+    static constexpr int KR = 16;
+    static constexpr int PS = KR / 2;
+    static constexpr int NCH = KR / 4;
+    static constexpr int MPS = NCH / 2;
     static constexpr int A_BYTES = BM * KR * 4;
     static constexpr int B_BYTES = BN * KR * 4;
     static constexpr int STAGE = A_BYTES + B_BYTES;
     static constexpr int B_COPY = B_BYTES;
-    static constexpr int NST = 16;  // 192 KB of stages: one CTA per SM
+    static constexpr int NST = (192 * 1024) / STAGE;
     static constexpr uint32_t IDESC =
         (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 };
+static_assert(Cfg<FDTD_N2F_BF16X3>::NST <= MAX_STAGE && Cfg<FDTD_N2F_TF32>::NST <= MAX_STAGE,
+              "stage ring larger than the barrier arrays");
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -344,19 +353,25 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                     }
                     tc_fence_after();
                     const uint32_t st = sbase + s * C::STAGE;
-                    if (MODE == FDTD_N2F_BF16X3) {
-                        const uint64_t ahi = make_desc(st, BM * 16, 128);
-                        const uint64_t alo = make_desc(st + C::A_BYTES, BM * 16, 128);
-                        const uint64_t bhi = make_desc(st + 2 * C::A_BYTES, BN * 16, 128);
-                        const uint64_t blo =
-                            make_desc(st + 2 * C::A_BYTES + C::B_BYTES, BN * 16, 128);
-                        mma<MODE>(d, ahi, bhi, ks > 0 ? 1u : 0u);
-                        mma<MODE>(d, ahi, blo, 1u);
-                        mma<MODE>(d, alo, bhi, 1u);
-                    } else {
-                        const uint64_t a = make_desc(st, BM * 16, 128);
-                        const uint64_t bb = make_desc(st + C::A_BYTES, BN * 16, 128);
-                        mma<MODE>(d, a, bb, ks > 0 ? 1u : 0u);
+#pragma unroll
+                    for (int m = 0; m < C::MPS; ++m) {
+                        // MMA m reads K chunks 2m and 2m+1 of the stage
+                        const uint32_t ao = m * 2 * (BM / 8) * 128, bo = m * 2 * (BN / 8) * 128;
+                        const uint32_t acc0 = (ks > 0 || m > 0) ? 1u : 0u;
+                        if (MODE == FDTD_N2F_BF16X3) {
+                            const uint64_t ahi = make_desc(st + ao, BM * 16, 128);
+                            const uint64_t alo = make_desc(st + C::A_BYTES + ao, BM * 16, 128);
+                            const uint64_t bhi = make_desc(st + 2 * C::A_BYTES + bo, BN * 16, 128);
+                            const uint64_t blo =
+                                make_desc(st + 2 * C::A_BYTES + C::B_BYTES + bo, BN * 16, 128);
+                            mma<MODE>(d, ahi, bhi, acc0);
+                            mma<MODE>(d, ahi, blo, 1u);
+                            mma<MODE>(d, alo, bhi, 1u);
+                        } else {
+                            const uint64_t a = make_desc(st + ao, BM * 16, 128);
+                            const uint64_t bb = make_desc(st + C::A_BYTES + bo, BN * 16, 128);
+                            mma<MODE>(d, a, bb, acc0);
+                        }
                     }
                     mma_commit(smem_u32(&sm->empty[s]));
                     last = g;
@@ -407,7 +422,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             }
             if (MODE == FDTD_N2F_BF16X3) {
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
+                for (int c = 0; c < C::NCH; ++c) {
                     // packed conversions: two values per cvt.rn.bf16x2.f32
                     __align__(16) __nv_bfloat162 hi[4], lo[4];
 #pragma unroll
@@ -424,7 +439,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                 }
             } else {
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
+                for (int c = 0; c < C::NCH; ++c) {
                     float4 v4 = make_float4(tf32_rna(vals[4 * c]), tf32_rna(vals[4 * c + 1]),
                                             tf32_rna(vals[4 * c + 2]), tf32_rna(vals[4 * c + 3]));
                     *reinterpret_cast<float4 *>(st + c * (BM / 8) * 128 + roff) = v4;
@@ -496,8 +511,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
 }
 
 // Pack the currents of one face into the tiled B operand: for every (frequency,
-// n tile, K step) a contiguous block [hi|lo][chunk 2][256 rows][16 bytes]
-// (BF16) or [chunk 2][256 rows][16 bytes] (TF32), rows n = (q_local*4 + c)*2 + ri_n,
+// n tile, K step) a contiguous block [hi|lo][chunk NCH][256 rows][16 bytes]
+// (BF16) or [chunk NCH][256 rows][16 bytes] (TF32), rows n = (q_local*4 + c)*2 + ri_n,
 // K index k = 2p + ri_k, value Re/−Im/Im/Re of cur[p][q][c] by (ri_k, ri_n);
 // zero outside [0, np) x [0, nq).
 template <int MODE, typename CT>
@@ -505,14 +520,14 @@ __global__ void k_n2f_pack(const CT *cur, int nfreq, int np, int nq, int KS, int
                            unsigned char *dst) {
     using C = Cfg<MODE>;
     constexpr int EPC = MODE == FDTD_N2F_BF16X3 ? 8 : 4;  // elements per 16-byte chunk
-    const int64_t nchunks = (int64_t)nfreq * NT * KS * 2 * BN;
+    const int64_t nchunks = (int64_t)nfreq * NT * KS * C::NCH * BN;
     for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q0 < nchunks;
          q0 += (int64_t)gridDim.x * blockDim.x) {
         int64_t t = q0;
         const int row = (int)(t % BN);
         t /= BN;
-        const int chunk = (int)(t % 2);
-        t /= 2;
+        const int chunk = (int)(t % C::NCH);
+        t /= C::NCH;
         const int ks = (int)(t % KS);
         t /= KS;
         const int nt = (int)(t % NT);
@@ -641,7 +656,8 @@ int k_real_per_step(int mode) {
 template <typename CT>
 cudaError_t launch_pack(int mode, const CT *cur, int nfreq, int np, int nq, int KS, int NT,
                         unsigned char *dst, cudaStream_t st) {
-    const int64_t n = (int64_t)nfreq * NT * KS * 2 * BN;
+    const int nch = mode == FDTD_N2F_BF16X3 ? Cfg<FDTD_N2F_BF16X3>::NCH : Cfg<FDTD_N2F_TF32>::NCH;
+    const int64_t n = (int64_t)nfreq * NT * KS * nch * BN;
     int64_t blocks = (n + 255) / 256;
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (mode == FDTD_N2F_BF16X3)
