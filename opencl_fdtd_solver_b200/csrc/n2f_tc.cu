@@ -14,15 +14,15 @@
 //
 // Kernel k_n2f_tc: one CTA per (128-direction tile, face, frequency), 6 + 4·NGRP warps.
 //   * warp 0: B producer.  B (currents, N × K) is pre-packed by k_n2f_pack in
-//     the K-major core-matrix layout, one contiguous 16 KB (8 KB) block per
-//     (n tile, K step), and moved with one cp.async.bulk per stage (no tensor
-//     map, no multicast).
+//     the K-major core-matrix layout, one contiguous 32 KB block per
+//     (n tile, K step) in both modes, and moved with one cp.async.bulk per
+//     stage (no tensor map, no multicast).
 //   * warp 1: one thread issues tcgen05.mma (kind::f16 BF16: hi·hi + hi·lo +
-//     lo·hi, or kind::tf32) into a 128 × 256 FP32 accumulator in TMEM,
-//     double-buffered across n tiles (512 columns).
+//     lo·hi, or kind::tf32), MPS K groups per stage (2 BF16, 4 TF32), into a 128 × 256 FP32
+//     accumulator in TMEM, double-buffered across n tiles (512 columns).
 //   * warps 2-5 and 10 onwards: A (phases, 128 × K), generated in shared memory
 //     per K step, one direction per thread, NGRP groups on interleaved stages: a
-//     float64 rotation times eight (four) precomputed float phases, split into
+//     float64 rotation times PS (16) precomputed float phases, split into
 //     bf16 hi + lo (or rounded to tf32), written in the K-major core-matrix
 //     layout.
 //   * warps 6-9: epilogue.  Each thread owns one TMEM lane (one direction),
@@ -73,7 +73,7 @@ struct Cfg<FDTD_N2F_BF16X3> {
 };
 template <>
 struct Cfg<FDTD_N2F_TF32> {
-    static constexpr int KR = 16;
+    static constexpr int KR = 32;
     static constexpr int PS = KR / 2;
     static constexpr int NCH = KR / 4;
     static constexpr int MPS = NCH / 2;
