@@ -772,6 +772,107 @@ def run_host_monitor_leg(args):
     return out
 
 
+# ------------------------------------------------------- medium-config legs
+MED_N, MED_NPML, MED_HALF = 256, 12, 44
+MED_FREQS = np.linspace(20e9, 40e9, 8)
+
+
+def medium_engine(box=True, fused=True):
+    """The medium configuration: 256³ FP32, npml 12, εr = 4 sphere (r = 40
+    cells), a rim-tapered Jx sheet at z = npml + 8 across the PML-free span, and
+    (``box``) the 6-face Huygens DFT box of half-width 44 cells at 8 frequencies."""
+    from opencl_fdtd_solver_b200 import CUDAFDTD, CUDANear2FarMonitor
+
+    n, npml, dl = MED_N, MED_NPML, 1e-3
+    shape = (n,) * 3
+    ii, jj, kk = np.meshgrid(*[np.arange(n)] * 3, indexing="ij", sparse=True)
+    eps = np.ones(shape, np.float32)
+    eps[(ii - n // 2) ** 2 + (jj - n // 2) ** 2 + (kk - n // 2) ** 2 < 40**2] = 4.0
+    g = CUDAFDTD(shape, dl, npml=npml, fused=fused)
+    g.set_epsilon(eps)
+    z = npml + 8
+    g.add_source(lambda f: f.add_source_Jx(z, gaussian_sine(f.t, 30e9, 20e9), npml, n - npml,
+                                           npml, n - npml, rim_taper=True))
+    mon = None
+    if box:
+        mon = CUDANear2FarMonitor(g, (n // 2 * dl,) * 3, (2 * MED_HALF * dl,) * 3, MED_FREQS)
+    return g, mon
+
+
+def run_huygens_leg(args):
+    """Cost of the Huygens-box face DFT (89³ box, 8 frequencies) on the medium
+    configuration: ms per step with and without the box monitor, device time by
+    CUDA events on the engine's stream and host wall time (the monitor's launch
+    is issued from its Python callback after each step).  The reference quotes
+    about 1.5 % for its fused 6-face DFT (README.md:192)."""
+    import torch
+
+    k = args.huygens_steps
+    out = {"workload": f"medium_{MED_N}^3_fp32_npml{MED_NPML}_sphere_sheet_box"
+                       f"{2 * MED_HALF + 1}^3_{MED_FREQS.size}freqs", "steps": k}
+    for tag, box in (("no_box", False), ("box", True)):
+        g, mon = medium_engine(box=box)
+        for _ in range(args.warmup):
+            g.step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(g.queue)
+        for _ in range(k):
+            g.step()
+        e1.record(g.queue)
+        torch.cuda.synchronize()
+        out[f"{tag}_wall_ms_per_step"] = round((time.perf_counter() - t0) / k * 1e3, 4)
+        out[f"{tag}_device_ms_per_step"] = round(e0.elapsed_time(e1) / k, 4)
+        del g, mon
+        torch.cuda.empty_cache()
+    for kind in ("wall", "device"):
+        a, b = out[f"no_box_{kind}_ms_per_step"], out[f"box_{kind}_ms_per_step"]
+        out[f"overhead_{kind}_pct"] = round(100.0 * (b - a) / a, 2)
+    out["reference_claim_pct"] = 1.5
+    return out
+
+
+def run_kernels_leg(args):
+    """One launch (after warm-up) of each auxiliary kernel at documented sizes,
+    timed by CUDA events; the workload of the per-kernel ncu summaries.
+      * medium configuration (256³, npml 12): one fused step with the Huygens box
+        (k_shell_H, k_interior, k_plane_dft_box, k_shell_E, k_dft_faces) and one
+        split step (k_update_H, k_update_E), with a z-plane DFT of Ex at 4 freqs;
+      * the far field of the box at one frequency onto 181 x 91 directions
+        (k_farfield_nl, k_farfield_eh);
+      * the tensor-core contraction of a 160³ box (6 faces, 4 currents, 8 freqs)
+        onto 361 x 181 directions in split-BF16 (k_n2f_pack, k_n2f_tc, k_n2f_combine)."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import CUDAPlaneDFTMonitor, near2far_contract
+
+    res = {}
+    g, mon = medium_engine(box=True)
+    CUDAPlaneDFTMonitor(g, "z", MED_N // 2, FREQS, ("Ex",))
+    for _ in range(args.warmup):
+        g.step()
+    st = g.queue
+    res["fused_step_with_box_ms"] = round(timed(g.step, st)[0], 4)
+    g._fused_enabled = False
+    res["split_step_with_box_ms"] = round(timed(g.step, st)[0], 4)
+    th = np.deg2rad(np.linspace(0.0, 180.0, 181))
+    ph = np.deg2rad(np.linspace(0.0, 180.0, 91, endpoint=False))
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    pts = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1).reshape(-1, 3)
+    res["farfield_direct_16471_ms"] = round(timed(lambda: mon.get_farfields(pts, 3), st)[0], 3)
+    del g, mon
+    torch.cuda.empty_cache()
+    faces = n2f_faces(160, 8)
+    dirs = n2f_directions()
+    freqs = np.linspace(10e9, 40e9, 8)
+    res["n2f_bf16x3_box160_8freqs_ms"] = round(
+        timed(lambda: near2far_contract(faces, freqs, dirs, mode="bf16x3"),
+              torch.cuda.current_stream())[0], 3)
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -795,11 +896,14 @@ def main(argv=None):
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 throughput leg")
     ap.add_argument("--fp64-size", type=int, default=384)
     ap.add_argument("--fp64-steps", type=int, default=100)
-    ap.add_argument("--only", choices=("n2f", "adjoint", "fp64", "host_monitor"),
+    ap.add_argument("--only", choices=("n2f", "adjoint", "fp64", "host_monitor", "huygens",
+                                       "kernels"),
                     help="run one auxiliary leg alone and print its object (profiling)")
     ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
     ap.add_argument("--n2f-freqs", type=int, default=32)
     ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS, help="time steps per adjoint solve")
+    ap.add_argument("--huygens-steps", type=int, default=500,
+                    help="timed steps of each arm of the Huygens-box overhead leg")
     ap.add_argument("--adj-fd-voxels", type=int, default=16,
                     help="design voxels checked by central differences")
     ap.add_argument("--cpu-budget", type=float, default=60.0,
@@ -817,7 +921,8 @@ def main(argv=None):
     rank, world, local = dist_setup(args.gpus)
     if args.only:
         res = {"n2f": run_n2f_leg, "adjoint": run_adjoint_leg, "fp64": run_fp64_leg,
-               "host_monitor": run_host_monitor_leg}[args.only](args)
+               "host_monitor": run_host_monitor_leg, "huygens": run_huygens_leg,
+               "kernels": run_kernels_leg}[args.only](args)
         if rank == 0:
             print(json.dumps({args.only: res}), flush=True)
         return 0

@@ -170,9 +170,12 @@ int fdtd_dft_rel_change(const double *cur, const double *prev, int32_t n_face,
  * pool set up at start-up.  Its partial sums live in a 16 KiB array inside
  * the library (held on every GPU that loads it until the process exits), so
  * n_face is limited to FDTD_NOALLOC_MAX_FACE; larger boxes get
- * FDTD_ERR_INVALID.  The first call on each device resolves that array's
- * device address, so make it before any stream capture.  Calls that overlap
- * on the GPU share the array and race.  No counterpart in the reference. */
+ * FDTD_ERR_INVALID.  Each call made outside a stream capture looks up that
+ * array's device address on the current device (so a device reset cannot
+ * leave a stale one); a call inside a capture reuses the device's last
+ * address, so make the first call on each device before any stream capture.
+ * Calls that overlap on the GPU share the array and race.  No counterpart in
+ * the reference. */
 #define FDTD_NOALLOC_MAX_FACE (1024 * 256)
 int fdtd_dft_rel_change_noalloc(const double *cur, const double *prev, int32_t n_face,
                                 int32_t nfreq, int32_t fi, double *out2, void *stream);
@@ -359,6 +362,19 @@ const char *fdtd_last_error(void);
  * read the flag; clears it when reset != 0.  No reference counterpart (the
  * reference kernels have no device-side waits). */
 int fdtd_device_status(int32_t *flags, int32_t reset);
+
+/* Budget of the bounded pipeline waits of one kernel, for later launches from
+ * this process: kernel FDTD_WAIT_INTERIOR (the fused step's interior kernel;
+ * budget in mbarrier polls, default and maximum 2^24) or FDTD_WAIT_N2F (the
+ * tensor-core near-to-far contraction; budget in nanoseconds, default 2e8).
+ * budget < 0 restores the default; 0 makes a wait give up unless its phase has
+ * already completed, which exercises the timeout path: the kernel raises its
+ * fdtd_device_status bit, still waits (with the default bound) for every copy
+ * and MMA it issued, frees what it holds and returns.  A launch that timed out
+ * leaves its outputs undefined.  No reference counterpart. */
+#define FDTD_WAIT_INTERIOR 0
+#define FDTD_WAIT_N2F 1
+int fdtd_set_wait_budget(int32_t kernel, int64_t budget);
 
 /* Library build tag, e.g. "fdtd_b200 sm_100a". */
 const char *fdtd_version(void);

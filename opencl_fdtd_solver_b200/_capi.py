@@ -32,6 +32,8 @@ FDTD_SRC_EX = 1
 FDTD_N2F_BF16X3 = 0
 FDTD_N2F_TF32 = 1
 FDTD_N2F_FP64 = 2
+FDTD_WAIT_INTERIOR = 0
+FDTD_WAIT_N2F = 1
 
 V3 = c_void_p * 3
 V6 = c_void_p * 6
@@ -134,6 +136,7 @@ SIGNATURES = {
                                     c_void_p]),
     "fdtd_last_error": (c_char_p, []),
     "fdtd_device_status": (c_int32, [POINTER(c_int32), c_int32]),
+    "fdtd_set_wait_budget": (c_int32, [c_int32, c_int64]),
     "fdtd_version": (c_char_p, []),
 }
 

@@ -38,17 +38,6 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found; set NVCC or put the CUDA toolkit on PATH")
 
 
-def cutlass_include() -> list[str]:
-    """CuTe/CUTLASS headers vendored in site-packages (used by the tensor-core kernels)."""
-    import site
-
-    for base in site.getsitepackages():
-        inc = Path(base) / "flashinfer" / "data" / "cutlass" / "include"
-        if (inc / "cute").is_dir():
-            return ["-I", str(inc)]
-    return []
-
-
 def build(force: bool = False, verbose: bool = False) -> Path:
     sources = sorted(CSRC.glob("*.cu"))
     headers = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
@@ -57,11 +46,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         return OUT
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
-    extra_inc = cutlass_include()
     objs = []
     for src in sources:
         obj = BUILD_DIR / (src.stem + ".o")
-        flags = list(COMMON) + extra_inc
+        flags = list(COMMON)
         if src.name in NO_FMA:
             flags.append("--fmad=false")
         cmd = [cc, *ARCH, *flags, "-c", str(src), "-o", str(obj)]

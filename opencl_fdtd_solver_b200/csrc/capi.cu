@@ -26,6 +26,7 @@ cudaError_t launch_farfield(const fdtd_box &b, const double *acc, int fi, double
                             double k_wave, double eta0, const double *obs, int n_obs,
                             double *nl, double *eh, cudaStream_t st);
 int read_fused_error(int reset);
+void set_interior_wait_polls(int64_t polls);
 cudaError_t launch_farfield_eh(const void *nl, int nl_f64, const double *obs, int n_obs,
                                double k_wave, double eta0, double *eh, cudaStream_t st);
 void profile_enable(bool on);
@@ -380,6 +381,16 @@ int fdtd_device_status(int32_t *flags, int32_t reset) {
     if (e != cudaSuccess) return cuda_status(e, "device_status");
     *flags = fdtd::read_fused_error(reset) | (fdtd::n2f::read_error(reset) ? 2 : 0);
     return cuda_status(cudaGetLastError(), "device_status");
+}
+
+int fdtd_set_wait_budget(int32_t kernel, int64_t budget) {
+    if (kernel == FDTD_WAIT_INTERIOR)
+        fdtd::set_interior_wait_polls(budget);
+    else if (kernel == FDTD_WAIT_N2F)
+        fdtd::n2f::set_wait_ns(budget);
+    else
+        return fail(FDTD_ERR_INVALID, "unknown wait-budget kernel %d", kernel);
+    return FDTD_OK;
 }
 
 int fdtd_update_H(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c, void *stream) {

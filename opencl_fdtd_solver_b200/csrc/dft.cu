@@ -336,29 +336,39 @@ cudaError_t launch_rel_change(const double *cur, const double *prev, int n, int 
 // Each call writes every partial it reads back, so nothing needs clearing
 // between calls; calls that overlap on the GPU share the array and race.
 constexpr int NOALLOC_REL_BLOCKS = 1024;
+static_assert(NOALLOC_REL_BLOCKS * REL_THREADS == FDTD_NOALLOC_MAX_FACE,
+              "the built-in scratch array must hold FDTD_NOALLOC_MAX_FACE face samples");
 static __device__ __align__(256) double g_rel_scratch[2 * NOALLOC_REL_BLOCKS];
 
 int noalloc_rel_max_face() { return NOALLOC_REL_BLOCKS * REL_THREADS; }
 
 namespace {
 std::mutex g_scratch_mu;
-double *g_scratch_ptr[256];  // device address of g_rel_scratch, per device ordinal
+double *g_scratch_ptr[256];  // last resolved device address of g_rel_scratch, per device
 }  // namespace
 
-// Device address of the scratch array on the current device.  The first call
-// on a device resolves it with cudaGetSymbolAddress (host code must not use the
-// array's name as a device pointer: it is only a host-side stand-in).
-cudaError_t noalloc_rel_scratch(double **out) {
+// Device address of the scratch array on the current device.  Host code must
+// not use the array's name as a device pointer (it is only a host-side
+// stand-in), so the address comes from cudaGetSymbolAddress, with that device
+// current.  It is looked up again on every call made while `st` is not being
+// captured, so a device reset (which reloads the module and may move the array)
+// cannot leave a stale address behind; during a capture the address from the
+// device's last uncaptured call is used, and a capture before any such call is
+// refused.
+cudaError_t noalloc_rel_scratch(cudaStream_t st, double **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return e;
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_rel_scratch);
-        if (e != cudaSuccess) return e;
+        if ((e = cudaGetSymbolAddress(&p, g_rel_scratch)) != cudaSuccess) return e;
         g_scratch_ptr[dev] = static_cast<double *>(p);
+    } else if (!g_scratch_ptr[dev]) {
+        return cudaErrorStreamCaptureUnsupported;
     }
     *out = g_scratch_ptr[dev];
     return cudaSuccess;
@@ -367,7 +377,7 @@ cudaError_t noalloc_rel_scratch(double **out) {
 cudaError_t launch_rel_change_noalloc(const double *cur, const double *prev, int n, int nfreq,
                                       int fi, double *out2, cudaStream_t st) {
     double *scratch = nullptr;
-    cudaError_t e = noalloc_rel_scratch(&scratch);
+    cudaError_t e = noalloc_rel_scratch(st, &scratch);
     if (e != cudaSuccess) return e;
     const int nb = (n + REL_THREADS - 1) / REL_THREADS;
     k_rel_partial<<<nb, REL_THREADS, 0, st>>>(reinterpret_cast<const double2 *>(cur),

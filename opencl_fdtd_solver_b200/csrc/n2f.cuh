@@ -30,6 +30,7 @@ struct Params {
     const unsigned char *btiles;
     float2 *partial;      // [nfreq][nfaces][n_obs][4]
     int comp_map[24];     // face-local current -> NL component (Nx Ny Nz Lx Ly Lz)
+    uint64_t wait_ns;     // budget of each pipeline wait (0: give up unless already complete)
 };
 
 size_t stage_smem(int mode);
@@ -43,6 +44,9 @@ cudaError_t launch_combine(const Params &P, int nfreq, float2 *nl, cudaStream_t 
 template <typename CT>
 cudaError_t launch_fp64(const Params &P, int nfreq, double2 *nl, cudaStream_t st);
 int read_error(int reset);
+// Wait budget of the contraction kernel's pipeline waits, in nanoseconds;
+// a negative value restores the default (0.2 s).  Drain waits keep 0.2 s.
+void set_wait_ns(int64_t ns);
 
 }  // namespace n2f
 }  // namespace fdtd

@@ -31,12 +31,14 @@
 // Complex arithmetic in real GEMM form: K interleaves (Re, Im) of u_p and N
 // interleaves (Re, Im) of T, with B = [[Br, Bi], [−Bi, Br]] per (p, (q, c)).
 //
-// Every mbarrier wait is bounded in wall time; on timeout the kernel raises bit
-// 1 of the device error flag, stops issuing, drains its own copies and MMAs
-// (bounded), frees TMEM and returns.
+// Every mbarrier wait is bounded in wall time (Params::wait_ns, 0.2 s by
+// default; fdtd_set_wait_budget lowers it); on timeout the kernel raises bit 1
+// of the device error flag, stops issuing, drains its own copies and MMAs (with
+// the default bound), frees TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "launch_count.cuh"
@@ -107,6 +109,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Non-blocking probe of a phase (no suspension), used by a zero wait budget.
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(bar), "r"(parity)
@@ -232,11 +246,20 @@ __device__ __forceinline__ uint64_t gtimer() {
     return t;
 }
 
-// Bounded wait shared by all roles: gives up after WAIT_NS of wall time, when
-// another role of this CTA aborted, or when another CTA raised the error flag.
-// Returns false in all three cases (and raises the flags on a timeout).
+// Bounded wait shared by all roles: gives up after `budget_ns` of wall time
+// (the launch's Params::wait_ns, 0.2 s unless a caller lowered it), when another
+// role of this CTA aborted, or when another CTA raised the error flag.  Returns
+// false in all three cases (and raises the flags on a timeout).  A zero budget
+// gives up at once unless the phase has already completed (non-blocking probe).
 constexpr uint64_t WAIT_NS = 200000000ull;  // 0.2 s; a normal wait is microseconds
-__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                         uint64_t budget_ns) {
+    if (budget_ns == 0) {
+        if (mbar_test_wait(bar, parity)) return true;
+        *abort_flag = 1;
+        atomicOr(&g_n2f_error, 1);
+        return false;
+    }
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = gtimer();
     uint32_t it = 0;
@@ -246,7 +269,7 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
                 *abort_flag = 1;
                 return false;
             }
-            if (gtimer() - t0 > WAIT_NS) {
+            if (gtimer() - t0 > budget_ns) {
                 *abort_flag = 1;
                 atomicOr(&g_n2f_error, 1);
                 return false;
@@ -315,7 +338,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             for (int g = 0; g < total; ++g) {
                 const int s = g % NSTAGE;
                 if (g >= NSTAGE &&
-                    !wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag))
+                    !wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag, P.wait_ns))
                     break;
                 const uint32_t bar = smem_u32(&sm->full_b[s]);
                 mbar_arrive_tx(bar, C::B_COPY);
@@ -337,7 +360,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             for (int nt = 0; nt < NT && ok; ++nt) {
                 const int b = nt & 1;
                 if (nt >= 2 &&
-                    !wait_bar(smem_u32(&sm->acc_empty[b]), ((nt >> 1) + 1) & 1, abort_flag)) {
+                    !wait_bar(smem_u32(&sm->acc_empty[b]), ((nt >> 1) + 1) & 1, abort_flag, P.wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -346,8 +369,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                 for (int ks = 0; ks < KS; ++ks) {
                     const int g = nt * KS + ks, s = g % NSTAGE;
                     const uint32_t par = (g / NSTAGE) & 1;
-                    if (!wait_bar(smem_u32(&sm->full_b[s]), par, abort_flag) ||
-                        !wait_bar(smem_u32(&sm->full_a[s]), par, abort_flag)) {
+                    if (!wait_bar(smem_u32(&sm->full_b[s]), par, abort_flag, P.wait_ns) ||
+                        !wait_bar(smem_u32(&sm->full_a[s]), par, abort_flag, P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -408,7 +431,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             if (ks <= prev_ks || prev_ks < 0) U = zphase_turns(gp, (double)(ks * C::PS));
             prev_ks = ks;
             if (g >= NSTAGE &&
-                !wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag))
+                !wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag, P.wait_ns))
                 break;
             unsigned char *st = stages + s * C::STAGE;
             const float2 uf = make_float2((float)U.x, (float)U.y);
@@ -472,7 +495,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                        make_float2(0.f, 0.f)};
         for (int nt = 0; nt < NT; ++nt) {
             const int b = nt & 1;
-            if (!wait_bar(smem_u32(&sm->acc_full[b]), (nt >> 1) & 1, abort_flag)) break;
+            if (!wait_bar(smem_u32(&sm->acc_full[b]), (nt >> 1) & 1, abort_flag, P.wait_ns)) break;
             tc_fence_after();
             const uint32_t base = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(b * BN);
 #pragma unroll 1
@@ -668,7 +691,15 @@ cudaError_t launch_pack(int mode, const CT *cur, int nfreq, int np, int nq, int 
     return cudaGetLastError();
 }
 
-cudaError_t launch_contract(int mode, const Params &P, int nfreq, cudaStream_t st) {
+namespace {
+std::atomic<long long> g_wait_ns{(long long)WAIT_NS};
+}
+
+void set_wait_ns(int64_t ns) { g_wait_ns.store(ns < 0 ? (long long)WAIT_NS : ns); }
+
+cudaError_t launch_contract(int mode, const Params &Pin, int nfreq, cudaStream_t st) {
+    Params P = Pin;
+    P.wait_ns = (uint64_t)g_wait_ns.load();
     const size_t smem = stage_smem(mode);
     dim3 grid((P.n_obs + BM - 1) / BM, P.nfaces, nfreq);
     cudaError_t e;

@@ -33,8 +33,10 @@
 //
 // Arithmetic is compiled with --fmad=false and follows the reference operand
 // order, so every cell equals the split kernels and the CPU oracle bit for bit.
-// Every mbarrier wait is bounded; on timeout the kernel raises a device error
-// flag, drains its outstanding copies (bounded again) and returns.
+// Every mbarrier wait is bounded (InteriorBox::wait_polls, WAIT_LIMIT polls by
+// default; fdtd_set_wait_budget lowers it); on timeout the kernel raises a
+// device error flag, drains the copies it issued (with the default bound) and
+// returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -42,6 +44,7 @@
 #include <vector>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstdint>
@@ -128,11 +131,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait: false (and the device error flag set) if the phase did not
-// complete within WAIT_LIMIT polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (unsigned it = 0; it < WAIT_LIMIT; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
+// complete within `limit` polls (the launch's InteriorBox::wait_polls,
+// WAIT_LIMIT unless a caller lowered it).  A zero limit gives up at once
+// unless the phase has already completed (non-blocking probe).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
+    if (limit == 0) {
+        if (mbar_test_wait(bar, parity)) return true;
+    } else {
+        for (unsigned it = 0; it < limit; ++it)
+            if (mbar_try_wait(bar, parity)) return true;
+    }
     atomicOr(&g_fused_error, 1);
     return false;
 }
@@ -168,6 +188,7 @@ __device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
 struct InteriorBox {
     int lo[3], hi[3];  // H box B = [lo, hi); E box B' = [lo+1, hi)
     int j0base, k0base, ntk, chunk;
+    unsigned wait_polls;  // budget of each pipeline wait (drains keep WAIT_LIMIT / 16)
     // dynamic shared memory layout (bytes)
     int stage_bytes, new_off, bar_off;
 };
@@ -218,8 +239,10 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     }
     __syncthreads();
 
+    int last_issued = pfirst - 1;  // thread 0 only: the last plane whose copies were issued
     auto issue = [&](int p) {
         const int s = (p - pfirst) % NSTAGE;
+        last_issued = p;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         if (p < plast) {
             mbar_expect_tx(&bar[s], L::tx_full(LOSSY));
@@ -266,7 +289,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     for (int p = pfirst; p < plast; ++p) {
         const int s = (p - pfirst) % NSTAGE, s1 = (p + 1 - pfirst) % NSTAGE;
         const uint32_t par = ((p - pfirst) / NSTAGE) & 1, par1 = ((p + 1 - pfirst) / NSTAGE) & 1;
-        const bool w = mbar_wait(&bar[s], par) && mbar_wait(&bar[s1], par1);
+        const bool w = mbar_wait(&bar[s], par, bx.wait_polls) &&
+                       mbar_wait(&bar[s1], par1, bx.wait_polls);
         if (!__syncthreads_and(w)) {  // CTA-uniform exit on a timed-out copy
             ok = false;
             break;
@@ -444,9 +468,13 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         if (tid == 0 && p + NSTAGE <= plast) issue(p + NSTAGE);
     }
     if (!ok) {
+        // drain: every copy issued must land before the CTA exits.  Only the
+        // last NSTAGE issued planes can still be in flight (earlier ones were
+        // consumed), and planes never issued are not waited for.
         __syncthreads();
         if (tid == 0) {
-            for (int p = pfirst; p <= plast; ++p) {
+            const int from = max(pfirst, last_issued - NSTAGE + 1);
+            for (int p = from; p <= last_issued; ++p) {
                 const int s = (p - pfirst) % NSTAGE;
                 const uint32_t par = ((p - pfirst) / NSTAGE) & 1;
                 for (unsigned it = 0; it < WAIT_LIMIT / 16; ++it)
@@ -524,6 +552,8 @@ bool make_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int el
     return true;
 }
 
+std::atomic<long long> g_wait_polls{(long long)WAIT_LIMIT};
+
 // Pipeline depth of the interior kernel: 4 stages (2 CTAs per SM) by default;
 // FDTD_B200_NSTAGE=3 selects 3 stages (3 CTAs per SM) as a tuning knob.
 int stage_count() {
@@ -591,6 +621,7 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
     bx.chunk = (nplanes + nchunk - 1) / nchunk;
     dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
     bx.stage_bytes = L::stage_bytes(a.lossy != 0);
+    bx.wait_polls = (unsigned)g_wait_polls.load();
     const int nstage = stage_count();
     bx.new_off = nstage * bx.stage_bytes;
     bx.bar_off = bx.new_off + L::NB;
@@ -780,6 +811,11 @@ template cudaError_t launch_step_fused<float>(const YeeArgs<float> &, const Sour
                                               const PlaneList &, cudaStream_t);
 template cudaError_t launch_step_fused<double>(const YeeArgs<double> &, const SourceList &,
                                                const PlaneList &, cudaStream_t);
+
+void set_interior_wait_polls(int64_t polls) {
+    g_wait_polls.store(polls < 0 ? (long long)WAIT_LIMIT
+                                 : (long long)(polls > (int64_t)WAIT_LIMIT ? WAIT_LIMIT : polls));
+}
 
 int read_fused_error(int reset) {
     int v = 0;

@@ -301,8 +301,14 @@ class CUDANear2FarMonitor:
 
         ``method="direct"`` (default) is the float64 surface sum per point, as the
         reference kernel does; ``"bf16x3"`` or ``"tf32"`` evaluates the surface sums
-        with the tensor-core contraction (``near2far_contract``; FP32 accumulation,
-        about 5e-6 / 3e-4 relative to the direct sums) and then the same second stage.
+        with the tensor-core contraction (``near2far_contract``, FP32 accumulation)
+        and then the same second stage.
+
+        Accuracy classes, as the maximum error over the peak of the float64 sums:
+        ``"bf16x3"`` stays within 1e-5 (about 5e-6 measured), the FP32-mode
+        tolerance of the far-field parity gate; ``"tf32"`` is about 3e-4 and is
+        *outside* that class (10 mantissa bits per operand): use it for previews
+        and sweeps, not for results held to 1e-5.
         """
         if method != "direct":
             return self._farfields_contract(obs_points, freq_index, method)

@@ -61,7 +61,9 @@ def near2far_contract(faces, freqs, directions, mode="bf16x3", *, stream=None):
     freqs      : frequencies (Hz), length nfreq
     directions : ``(n_obs, 3)`` directions (normalised here)
     mode       : ``"bf16x3"`` or ``"tf32"`` (tensor cores, complex64 result) or
-                 ``"fp64"`` (float64 direct sum, complex128 result)
+                 ``"fp64"`` (float64 direct sum, complex128 result).  Error against
+                 the float64 sums, over their peak: ``"bf16x3"`` ≤ 1e-5 (about 5e-6
+                 measured); ``"tf32"`` about 3e-4, outside the 1e-5 class.
     """
     if mode not in MODES:
         raise ValueError(f"mode must be one of {sorted(MODES)}, got {mode!r}")

@@ -16,44 +16,46 @@ from typing import Any, Callable, Protocol, runtime_checkable
 
 @runtime_checkable
 class StepCallback(Protocol):
-    """Callable invoked once per timestep with the solver instance.
+    """Anything callable as ``cb(engine)``; the engine calls it once per step.
 
-    Sources run after the H update and before the E update.
-    Monitors run after the full Yee step (fields and ``t`` advanced).
+    Registered as a source, it is called between the two half steps: H is already
+    at n+1/2 and ``engine.t`` reads the half-step time.  Registered as a monitor,
+    it is called once the step is complete, with E at n+1 and ``t`` advanced.
     """
 
     def __call__(self, fdtd: Any) -> None: ...
 
 
 class SourceMonitorMixin:
-    """Registration API for per-step sources and monitors.
+    """``add_source`` / ``add_monitor`` and their ``clear_*`` counterparts.
 
-    Concrete solvers initialise ``_sources`` and ``_monitors`` in ``__init__``.
+    An engine using this mixin owns two lists, ``_sources`` and ``_monitors``,
+    created in its constructor; the methods only append to or empty them.
     """
 
     _sources: list
     _monitors: list
 
     def add_source(self, source: StepCallback) -> StepCallback:
-        """Register ``source(fdtd)``; it runs after every H update."""
+        """Append ``source``, called with the engine between the H and E half steps."""
         if not callable(source):
             raise TypeError(f"source must be callable, got {type(source)!r}")
         self._sources.append(source)
         return source
 
     def add_monitor(self, monitor: StepCallback) -> StepCallback:
-        """Register ``monitor(fdtd)``; it runs after every full step."""
+        """Append ``monitor``, called with the engine at the end of each step."""
         if not callable(monitor):
             raise TypeError(f"monitor must be callable, got {type(monitor)!r}")
         self._monitors.append(monitor)
         return monitor
 
     def clear_sources(self) -> None:
-        """Remove all registered source callbacks."""
+        """Forget every source added so far."""
         self._sources.clear()
 
     def clear_monitors(self) -> None:
-        """Remove all registered monitor callbacks."""
+        """Forget every monitor added so far."""
         self._monitors.clear()
 
 

@@ -3,7 +3,9 @@
 Run in a container where the reference tree is present (it is not needed on a GPU
 host; the fixtures it writes are committed)::
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
+
+(``--reference`` defaults to the ``FDTD_REFERENCE_ROOT`` environment variable.)
 
 Outputs:
 
@@ -26,6 +28,7 @@ Outputs:
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import types
 import warnings
@@ -177,7 +180,9 @@ def host_monitor_cases(ref):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FDTD_REFERENCE_ROOT"),
+                    required="FDTD_REFERENCE_ROOT" not in os.environ,
+                    help="reference checkout (default: $FDTD_REFERENCE_ROOT)")
     ap.add_argument("--only", choices=("host_monitor",), default=None,
                     help="write just this fixture")
     args = ap.parse_args(argv)

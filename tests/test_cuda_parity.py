@@ -566,4 +566,5 @@ def test_medium_config_sphere_box_farfield(cuda, steps):
         t = mg.get_farfields(pts, fi, method="bf16x3")
         scale = np.abs(ref).max()
         assert np.abs(d - ref).max() <= 1e-9 * scale, fi
-        assert np.abs(t - ref).max() <= 5e-5 * scale, fi
+        # split-BF16 is held to the FP32-mode far-field tolerance, 1e-5 of peak
+        assert np.abs(t - ref).max() <= 1e-5 * scale, fi

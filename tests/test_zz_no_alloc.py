@@ -17,6 +17,8 @@ already run every other test.
 from __future__ import annotations
 
 import ctypes
+import re
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -74,10 +76,48 @@ def test_noalloc_rel_change_matches_caller_buffer_twice(setup):
         g.run(5)  # the next call sees new data, and the array still holds this call's sums
 
 
+def _header_capacity():
+    """FDTD_NOALLOC_MAX_FACE as the C header defines it (the library's own
+    static_assert ties its built-in array to the same macro)."""
+    hdr = (Path(__file__).resolve().parents[1] / "include" / "fdtd_b200.h").read_text()
+    m = re.search(r"#define\s+FDTD_NOALLOC_MAX_FACE\s+\(([^)]*)\)", hdr)
+    assert m, "FDTD_NOALLOC_MAX_FACE not found in include/fdtd_b200.h"
+    return int(eval(m.group(1), {"__builtins__": {}}))
+
+
+def test_noalloc_at_exact_capacity_matches_caller_buffer(setup):
+    """A box of exactly FDTD_NOALLOC_MAX_FACE samples uses every partial the
+    built-in array holds; two calls on different data both match the
+    caller-buffer entry point."""
+    torch, _, _, capi = setup
+    n = _header_capacity()
+    assert capi.FDTD_NOALLOC_MAX_FACE == n
+    nfreq = 2
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(99)
+    out = torch.empty(2, dtype=torch.float64, device="cuda")
+    ref = torch.empty(2, dtype=torch.float64, device="cuda")
+    nblk = int(capi.lib().fdtd_rel_change_blocks(n))
+    scratch = torch.empty(2 * nblk, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        cur = torch.randn((6, nfreq, n, 2), dtype=torch.float64, device="cuda", generator=gen)
+        prev = cur + 1e-3 * (call + 1) * torch.randn(cur.shape, dtype=torch.float64,
+                                                     device="cuda", generator=gen)
+        for fi in range(nfreq):
+            capi.run("fdtd_dft_rel_change", cur.data_ptr(), prev.data_ptr(), n, nfreq, fi,
+                     scratch.data_ptr(), ref.data_ptr(), None)
+            capi.run("fdtd_dft_rel_change_noalloc", cur.data_ptr(), prev.data_ptr(), n, nfreq,
+                     fi, out.data_ptr(), None)
+            torch.cuda.synchronize()
+            a, b = out.cpu().numpy(), ref.cpu().numpy()
+            assert b[0] > 0 and b[1] > 0, (call, fi, b)
+            np.testing.assert_allclose(a, b, rtol=1e-12, atol=0.0)
+
+
 def test_noalloc_rejects_boxes_beyond_capacity(setup):
     torch, _, _, capi = setup
     dummy = torch.zeros(2, dtype=torch.float64, device="cuda")
-    too_many = capi.FDTD_NOALLOC_MAX_FACE + 1
+    too_many = _header_capacity() + 1
     rc = capi.call("fdtd_dft_rel_change_noalloc", dummy.data_ptr(), dummy.data_ptr(), too_many,
                    1, 0, dummy.data_ptr(), None)
     assert rc == capi.FDTD_ERR_INVALID
