@@ -209,14 +209,18 @@ def make_engine(size, npml, dtype, fused=True):
 
 
 def cpu_engine(size, npml, dtype, backend):
-    """The same grid on the CPU (reference kernels compiled as C, or the oracle port)."""
+    """The same grid and step on the CPU (reference kernels compiled as C, or the
+    oracle port), with the same z-plane DFT of Ex at 4 frequencies (the oracle's
+    plane-DFT monitor: the reference has no plane-DFT kernel)."""
     from oracle.cpu_fdtd import OracleFDTD
+    from oracle.dft_oracle import OraclePlaneDFTMonitor
 
     shape = (size, size, size)
     o = OracleFDTD(shape, 1e-3, npml=npml, dtype=dtype, backend=backend)
     o.set_epsilon(blocky_eps(shape))
     c = size // 2
     o.add_source(lambda f: f.add_source_Jx(c, gaussian_pulse(f.t), i0=c, i1=c + 1, j0=c, j1=c + 1))
+    o._bench_dft = OraclePlaneDFTMonitor(o, "z", c, FREQS, ("Ex",))
     return o
 
 
@@ -234,6 +238,14 @@ def cpu_reference_rate(size, npml, dtype, seconds, backend):
         if el >= seconds or n >= 50:
             break
     return size**3 * n / el / 1e6, n, el, num_threads()
+
+
+def workload_config(size, npml, world):
+    """The workload both arms time (identical dicts, so the two lines compare)."""
+    return {"workload": f"yee_cpml_{size}^3_fp32_npml{npml}_blocky_eps_jx_point_zdft4",
+            "grid": [size] * 3, "npml": npml, "plane_dft_freqs_hz": list(FREQS),
+            "eps_seed": 1234, "l2": "inputs (~9 GB/step) exceed L2; no flush",
+            "parallelism": f"replicas{world}"}
 
 
 def run_reference_arm(args, rank, world):
@@ -268,11 +280,10 @@ def run_reference_arm(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(args.size**3 / value / 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"yee_cpml_{args.size}^3_fp32_npml{args.npml}_blocky_eps_jx_point_zdft4",
-                   "grid": [args.size] * 3, "npml": args.npml, "eps_seed": 1234,
-                   "cpu": True,
-                   "note": "the reference's Yee/CPML and source kernels on the host cores; the "
-                           "plane DFT has no reference kernel and is not part of this arm's step"},
+        "config": workload_config(args.size, args.npml, world),
+        "arm": "the reference's Yee/CPML and source kernels on the host cores, with the same "
+               "z-plane DFT of Ex at 4 frequencies (the oracle's plane-DFT monitor; the reference "
+               "has no plane-DFT kernel)",
         "cpu_baseline": {"value": round(value, 2), "unit": "Mcell/s", "cores": thr, "kind": kind,
                          "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "Mcell/s", "h2d_bytes_per_step": 0,
@@ -327,12 +338,12 @@ def run_steps_timed(g, k):
     torch.cuda.synchronize()
     capi.run("fdtd_profile_steps", 0)
     launches = lib.fdtd_launch_count() - n0
-    ms = (ctypes.c_double * 4)()
+    ms = (ctypes.c_double * 5)()
     nsteps = ctypes.c_int32()
     capi.run("fdtd_profile_read", ms, ctypes.byref(nsteps))
     per_kernel = {name: ms[i] / max(1, nsteps.value)
-                  for i, name in enumerate(("k_shell_H", "k_interior", "k_plane_dft_box",
-                                            "k_shell_E"))}
+                  for i, name in enumerate(("k_shell_H", "k_shell_E_outer", "k_interior",
+                                            "k_plane_dft_box", "k_shell_E_rim"))}
     phases = {f"ms_per_step_first_{split}": round(start.elapsed_time(mid) / max(1, split), 4)}
     if k > split:
         phases[f"ms_per_step_after_{split}"] = round(mid.elapsed_time(end) / (k - split), 4)
@@ -432,11 +443,8 @@ def run_b200_arm(args, rank, world, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"yee_cpml_{size}^3_fp32_npml{npml}_blocky_eps_jx_point_zdft4",
-                   "grid": list(shape), "npml": npml, "plane_dft_freqs_hz": list(FREQS),
-                   "eps_seed": 1234, "fused_step": fused,
-                   "l2": "inputs (~9 GB/step) exceed L2; no flush",
-                   "parallelism": f"replicas{world}"},
+        "config": workload_config(size, npml, world),
+        "fused_step": fused,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic, "peak_source": peak_kind,
@@ -463,6 +471,14 @@ def run_b200_arm(args, rank, world, local):
     if not args.no_n2f:
         barrier(world)
         line["n2f"] = run_n2f_leg(args)
+    if not args.no_fp64_error:
+        barrier(world)
+        line["fp64_error"] = run_fp64_error_leg(args)
+    if not args.no_huygens:
+        barrier(world)
+        line["huygens_box"] = run_huygens_leg(args)
+    if rank == 0 and world == 1 and not args.no_cpu and not args.no_numpy:
+        line["cpu_baseline_numpy"] = run_numpy_leg(args)
     return line
 
 
@@ -772,12 +788,162 @@ def run_host_monitor_leg(args):
     return out
 
 
+# ------------------------------------------------------- NumPy CPU baseline
+def numpy_rate(size, npml, courant, eps, warm, windows, per_window):
+    """Mcell/s of the NumPy face-CPML engine (the reference's NumPy algorithm,
+    restated bit-identically in ``oracle/numpy_face_cpml.py``): warm-up steps,
+    then ``windows`` timed windows of ``per_window`` steps, median
+    (reference ``benchmarks/benchmark_vs_meep.py:108-122``)."""
+    from oracle.numpy_face_cpml import NumPyFaceCPML
+
+    shape = (size,) * 3
+    o = NumPyFaceCPML(shape, 1e-3, npml=npml, courant=courant)
+    if eps is not None:
+        o.set_epsilon(eps)
+    c = size // 2
+    o.add_source(lambda f: f.add_source_Jx(c, gaussian_pulse(f.t), i0=c, i1=c + 1, j0=c, j1=c + 1))
+    o.run(warm)
+    rates = []
+    for _ in range(windows):
+        t0 = time.perf_counter()
+        o.run(per_window)
+        rates.append(size**3 * per_window / (time.perf_counter() - t0) / 1e6)
+    return statistics.median(rates), rates
+
+
+def run_numpy_leg(args):
+    """The reference's NumPy engine (face-striped CPML) on the host: the small
+    configuration's 64³ grid (2 warm-up steps, 3 windows of 10) and the 512³
+    roofline grid (1 warm-up step, 3 windows of 1 step; full-length NumPy runs
+    at 512³ take hours).  NumPy evaluates each array operation on one core."""
+    r64, w64 = numpy_rate(64, 8, 0.5, None, 2, 3, 10)
+    out = {"kind": "port", "engine": "NumPyFDTD_FaceCPML algorithm (oracle/numpy_face_cpml.py, "
+                                      "bit-identical to the reference on its fixtures)",
+           "threads": 1, "host_cpus": os.cpu_count(),
+           "omp_num_threads": os.environ.get("OMP_NUM_THREADS"),
+           "small_64^3": {"value": round(r64, 2), "unit": "Mcell/s",
+                          "windows_mcells": [round(x, 2) for x in w64],
+                          "sample": "64^3 FP32 vacuum, npml 8, Courant 0.5, 2 warm-up + 3 x 10 steps"}}
+    if not args.numpy_small_only:
+        shape = (args.size,) * 3
+        r512, w512 = numpy_rate(args.size, args.npml, None, blocky_eps(shape), 1, 3, 1)
+        out[f"roofline_{args.size}^3"] = {
+            "value": round(r512, 2), "unit": "Mcell/s", "windows_mcells": [round(x, 2) for x in w512],
+            "sample": f"{args.size}^3 FP32 blocky eps, npml {args.npml}, 1 warm-up + 3 x 1 step"}
+    return out
+
+
+# ------------------------------------------------------ FP32 vs FP64 errors
+def _peak_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.abs(a.astype(np.complex128 if np.iscomplexobj(a) else np.float64) - b).max()
+                 / np.abs(b).max())
+
+
+def run_fp64_error_leg(args):
+    """Each FP32 result's peak-normalised error against an FP64 run of the same
+    configuration (``max|x32 - x64| / max|x64|``):
+      * small (64³, npml 8, Courant 0.5, Jx point, 500 steps): Ex, Hy and their
+        z = 32 plane DFTs at 25/30/35 GHz, against the FP64 NumPy face-CPML engine;
+      * medium (256³ sphere, rim-tapered sheet, 2000 steps): the 8-frequency box
+        DFTs and the far field at 20 and 40 GHz (direct and split-BF16), against
+        the FP64 CUDA engine (itself within 1e-12 of FP64 NumPy on the parity tests);
+      * roofline (512³ blocky εr): the six fields and the Ex plane DFT after
+        ``--fp64-error-steps`` steps, against the FP64 CUDA engine."""
+    import torch
+
+    from opencl_fdtd_solver_b200 import CUDAFDTD, CUDAPlaneDFTMonitor
+    from oracle.numpy_face_cpml import NumPyFaceCPML
+
+    out = {}
+    # small configuration
+    freqs = [25e9, 30e9, 35e9]
+    g = CUDAFDTD((64,) * 3, 1e-3, npml=8, courant=0.5)
+    src = lambda f: f.add_source_Jx(32, gaussian_sine(f.t, 30e9, 20e9), i0=32, i1=33, j0=32,
+                                    j1=33)
+    g.add_source(src)
+    m = CUDAPlaneDFTMonitor(g, "z", 32, freqs, ("Ex", "Hy"))
+    g.run(500)
+    o = NumPyFaceCPML((64,) * 3, 1e-3, npml=8, dtype=np.float64, courant=0.5)
+    o.add_source(src)
+    om = 2 * np.pi * np.array(freqs)
+    acc = {c: np.zeros((3, 64, 64), np.complex128) for c in ("Ex", "Hy")}
+    st = {"p": None}
+
+    def plane(f):
+        st["p"] = (np.exp(1j * om * f.t) * f.dt if st["p"] is None
+                   else st["p"] * np.exp(1j * om * f.dt))
+        ph = st["p"] * np.exp(-0.5j * om * f.dt)
+        acc["Ex"] += st["p"][:, None, None] * f.Ex[:, :, 32][None]
+        acc["Hy"] += ph[:, None, None] * f.Hy[:, :, 32][None]
+
+    o.add_monitor(plane)
+    o.run(500)
+    out["small_64^3_500steps_vs_fp64_numpy"] = {
+        "Ex": _peak_err(g.Ex, o.Ex), "Hy": _peak_err(g.Hy, o.Hy),
+        "dft_Ex": _peak_err(m.dft("Ex"), acc["Ex"]), "dft_Hy": _peak_err(m.dft("Hy"), acc["Hy"])}
+    del g, m, o
+    torch.cuda.empty_cache()
+    # medium configuration
+    th = np.deg2rad(np.linspace(0.0, 180.0, 181))
+    ph_ = np.deg2rad(np.linspace(0.0, 180.0, 91, endpoint=False))
+    T, P = np.meshgrid(th, ph_, indexing="ij")
+    pts = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], -1).reshape(-1, 3)
+    res = {}
+    for dt_ in (np.float32, np.float64):
+        gm, mon = medium_engine(box=True, dtype=dt_)
+        gm.run(args.fp64_error_medium_steps)
+        r = {"box": [mon.face_dft(fi) for fi in range(MED_FREQS.size)],
+             "ff": {fi: mon.get_farfields(pts, fi) for fi in (0, MED_FREQS.size - 1)}}
+        if dt_ == np.float32:
+            r["ff_bf16x3"] = {fi: mon.get_farfields(pts, fi, method="bf16x3")
+                              for fi in (0, MED_FREQS.size - 1)}
+        res[dt_] = r
+        del gm, mon
+        torch.cuda.empty_cache()
+    a, b = res[np.float32], res[np.float64]
+    box_err = max(_peak_err(a["box"][fi][c], b["box"][fi][c])
+                  for fi in range(MED_FREQS.size) for c in a["box"][fi])
+    out[f"medium_{MED_N}^3_{args.fp64_error_medium_steps}steps_vs_fp64_cuda"] = {
+        "box_dft_max_over_freqs_components": box_err,
+        "farfield_direct": {f"{MED_FREQS[fi] / 1e9:.0f}GHz": _peak_err(a["ff"][fi], b["ff"][fi])
+                            for fi in a["ff"]},
+        "farfield_bf16x3": {f"{MED_FREQS[fi] / 1e9:.0f}GHz": _peak_err(a["ff_bf16x3"][fi],
+                                                                       b["ff"][fi])
+                            for fi in a["ff"]}}
+    # roofline grid
+    n, k = args.size, args.fp64_error_steps
+    shape = (n,) * 3
+    eps = blocky_eps(shape)
+    ref = None
+    errs = {}
+    for dt_ in (np.float64, np.float32):  # FP64 first; its fields stay on the device
+        gr, mr = make_engine(n, args.npml, dt_)
+        gr.set_epsilon(eps)
+        gr.run(k)
+        cur = {f: gr.field_tensor(f).double() for f in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
+        dft = mr.dft("Ex")
+        if ref is None:
+            ref = ({f: t.clone() for f, t in cur.items()}, dft)
+        else:
+            for f, t in cur.items():
+                errs[f] = float((t - ref[0][f]).abs().max() / ref[0][f].abs().max())
+            errs["dft_Ex"] = _peak_err(dft, ref[1])
+        del gr, mr, cur
+        torch.cuda.empty_cache()
+    del ref
+    torch.cuda.empty_cache()
+    out[f"roofline_{n}^3_{k}steps_vs_fp64_cuda"] = errs
+    return out
+
+
 # ------------------------------------------------------- medium-config legs
 MED_N, MED_NPML, MED_HALF = 256, 12, 44
 MED_FREQS = np.linspace(20e9, 40e9, 8)
 
 
-def medium_engine(box=True, fused=True):
+def medium_engine(box=True, fused=True, dtype=np.float32):
     """The medium configuration: 256³ FP32, npml 12, εr = 4 sphere (r = 40
     cells), a rim-tapered Jx sheet at z = npml + 8 across the PML-free span, and
     (``box``) the 6-face Huygens DFT box of half-width 44 cells at 8 frequencies."""
@@ -788,7 +954,7 @@ def medium_engine(box=True, fused=True):
     ii, jj, kk = np.meshgrid(*[np.arange(n)] * 3, indexing="ij", sparse=True)
     eps = np.ones(shape, np.float32)
     eps[(ii - n // 2) ** 2 + (jj - n // 2) ** 2 + (kk - n // 2) ** 2 < 40**2] = 4.0
-    g = CUDAFDTD(shape, dl, npml=npml, fused=fused)
+    g = CUDAFDTD(shape, dl, npml=npml, dtype=dtype, fused=fused)
     g.set_epsilon(eps)
     z = npml + 8
     g.add_source(lambda f: f.add_source_Jx(z, gaussian_sine(f.t, 30e9, 20e9), npml, n - npml,
@@ -894,14 +1060,24 @@ def main(argv=None):
                     help="skip the adjoint-gradient leg (t_grad / t_forward, FD check)")
     ap.add_argument("--no-n2f", action="store_true", help="skip the near-to-far contraction leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 throughput leg")
+    ap.add_argument("--no-huygens", action="store_true", help="skip the Huygens-box overhead leg")
     ap.add_argument("--fp64-size", type=int, default=384)
     ap.add_argument("--fp64-steps", type=int, default=100)
     ap.add_argument("--only", choices=("n2f", "adjoint", "fp64", "host_monitor", "huygens",
-                                       "kernels"),
+                                       "kernels", "numpy", "fp64_error"),
                     help="run one auxiliary leg alone and print its object (profiling)")
     ap.add_argument("--n2f-size", type=int, default=320, help="box edge (samples per face side)")
     ap.add_argument("--n2f-freqs", type=int, default=32)
     ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS, help="time steps per adjoint solve")
+    ap.add_argument("--no-numpy", action="store_true", help="skip the NumPy CPU-baseline leg")
+    ap.add_argument("--numpy-small-only", action="store_true",
+                    help="NumPy CPU baseline at 64^3 only (skip the 512^3 sample)")
+    ap.add_argument("--no-fp64-error", action="store_true",
+                    help="skip the FP32-vs-FP64 error leg")
+    ap.add_argument("--fp64-error-steps", type=int, default=1200,
+                    help="steps of the 512^3 FP32-vs-FP64 comparison")
+    ap.add_argument("--fp64-error-medium-steps", type=int, default=2000,
+                    help="steps of the medium-configuration FP32-vs-FP64 comparison")
     ap.add_argument("--huygens-steps", type=int, default=500,
                     help="timed steps of each arm of the Huygens-box overhead leg")
     ap.add_argument("--adj-fd-voxels", type=int, default=16,
@@ -922,7 +1098,8 @@ def main(argv=None):
     if args.only:
         res = {"n2f": run_n2f_leg, "adjoint": run_adjoint_leg, "fp64": run_fp64_leg,
                "host_monitor": run_host_monitor_leg, "huygens": run_huygens_leg,
-               "kernels": run_kernels_leg}[args.only](args)
+               "kernels": run_kernels_leg, "numpy": run_numpy_leg,
+               "fp64_error": run_fp64_error_leg}[args.only](args)
         if rank == 0:
             print(json.dumps({args.only: res}), flush=True)
         return 0

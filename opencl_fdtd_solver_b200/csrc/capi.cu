@@ -30,7 +30,7 @@ void set_interior_wait_polls(int64_t polls);
 cudaError_t launch_farfield_eh(const void *nl, int nl_f64, const double *obs, int n_obs,
                                double k_wave, double eta0, double *eh, cudaStream_t st);
 void profile_enable(bool on);
-cudaError_t profile_read(double ms[4], int *steps);
+cudaError_t profile_read(double ms[5], int *steps);
 struct MatScalars {
     double scale, dt, two_eps0, eps0;
 };
@@ -627,7 +627,7 @@ int fdtd_profile_steps(int32_t enable) {
     return FDTD_OK;
 }
 
-int fdtd_profile_read(double ms[4], int32_t *nsteps) {
+int fdtd_profile_read(double ms[5], int32_t *nsteps) {
     if (!ms || !nsteps) return fail(FDTD_ERR_INVALID, "NULL output");
     int n = 0;
     cudaError_t e = fdtd::profile_read(ms, &n);

@@ -1,18 +1,24 @@
 // Fused Yee step for sm_100a: one pass over HBM for the interior of the grid.
 //
-// Schedule of fdtd_step (three launches on one stream):
+// Schedule of fdtd_step (five launches on two streams):
+//   side stream, forked from the caller's stream:
 //   1. k_shell_H   (yee_shell.cu): H^{n+1/2} on the CPML shell outside the box
 //                  B = [npml, N-npml)^3, psi_H in place, into H_next.
-//   2. k_interior  (this file): H^{n+1/2} on B and E^{n+1} on B' = [npml+1,
+//   2. k_shell_E   (yee_shell.cu): E^{n+1} of the cells outside R = [npml,
+//                  N-npml+1)^3, whose stencils read H only outside B, with the
+//                  injections and plane DFTs of those cells.
+//   caller's stream, concurrently:
+//   3. k_interior  (this file): H^{n+1/2} on B and E^{n+1} on B' = [npml+1,
 //                  N-npml)^3, into H_next / E_next, sheet injections of those
 //                  cells in the E epilogue.  Every H value its E
 //                  stencil needs lies in B and is recomputed here, so it never
 //                  waits for the shell.
-//   3. k_plane_dft_box (yee_shell.cu, only with plane DFT monitors): the DFTs of
+//   then, after joining the side stream:
+//   4. k_plane_dft_box (yee_shell.cu, only with plane DFT monitors): the DFTs of
 //                  the monitored planes' cells inside B', read back from the
 //                  values just written (one plane, not a field pass).
-//   4. k_shell_E   (yee_shell.cu): E^{n+1} outside B' from the final H_next,
-//                  with the injections and plane DFTs of those cells.
+//   5. k_shell_E   (yee_shell.cu): E^{n+1} of the one-cell rim R \ B', whose
+//                  stencils read H of B, with its injections and plane DFTs.
 //
 // Interior kernel.  Each CTA owns a (TJ x TK) tile of (j, k) and marches along
 // i over a chunk of planes.  Plane p is brought into shared memory by TMA
@@ -650,11 +656,13 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
 
 // ---- per-launch timing of the step (diagnostics) ---------------------------
 namespace {
+constexpr int NEV = 7;
+constexpr int NPROF = 5;
 struct StepProfiler {
     std::mutex mu;
     bool on = false;
-    std::vector<std::array<cudaEvent_t, 6>> pending;
-    double ms[4] = {0.0, 0.0, 0.0, 0.0};
+    std::vector<std::array<cudaEvent_t, NEV>> pending;
+    double ms[NPROF] = {0.0, 0.0, 0.0, 0.0, 0.0};
     int steps = 0;
 };
 StepProfiler g_prof;
@@ -663,11 +671,11 @@ StepProfiler g_prof;
 cudaError_t prof_flush_locked() {
     cudaError_t err = cudaSuccess;
     for (auto &ev : g_prof.pending) {
-        // ev: 0 start, 1 shell H done (side stream), 2 interior done, 3 joined,
-        // 4 plane DFT done, 5 shell E done
-        cudaError_t e = cudaEventSynchronize(ev[5]);
-        const int from[4] = {0, 0, 3, 4}, to[4] = {1, 2, 4, 5};
-        for (int s = 0; s < 4 && e == cudaSuccess; ++s) {
+        // ev: 0 start, 1 shell H done (side stream), 2 outer shell E done (side),
+        // 3 interior done, 4 joined, 5 plane DFT done, 6 rim E done
+        cudaError_t e = cudaEventSynchronize(ev[6]);
+        const int from[NPROF] = {0, 1, 0, 4, 5}, to[NPROF] = {1, 2, 3, 5, 6};
+        for (int s = 0; s < NPROF && e == cudaSuccess; ++s) {
             float t = 0.f;
             e = cudaEventElapsedTime(&t, ev[from[s]], ev[to[s]]);
             g_prof.ms[s] += t;
@@ -680,10 +688,10 @@ cudaError_t prof_flush_locked() {
     return err;
 }
 
-bool prof_begin(std::array<cudaEvent_t, 6> &ev) {
+bool prof_begin(std::array<cudaEvent_t, NEV> &ev) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     if (!g_prof.on) return false;
-    for (int s = 0; s < 6; ++s)
+    for (int s = 0; s < NEV; ++s)
         if (cudaEventCreate(&ev[s]) != cudaSuccess) {
             for (int q = 0; q < s; ++q) cudaEventDestroy(ev[q]);
             return false;
@@ -691,16 +699,17 @@ bool prof_begin(std::array<cudaEvent_t, 6> &ev) {
     return true;
 }
 
-void prof_end(const std::array<cudaEvent_t, 6> &ev) {
+void prof_end(const std::array<cudaEvent_t, NEV> &ev) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     g_prof.pending.push_back(ev);
     if (g_prof.pending.size() >= 2048) prof_flush_locked();
 }
 // Side stream (per host thread and device) on which the CPML-shell H kernel
-// runs concurrently with the interior kernel: the two are independent (the
-// interior kernel recomputes every H it needs from E and H), so the latency-
-// bound shell fills the bandwidth the interior kernel leaves.  Joined back to
-// the caller's stream by an event before the E half.
+// and the outer shell-E kernel run concurrently with the interior kernel: they
+// are independent of it (the interior kernel recomputes every H it needs from E
+// and H, and the outer E cells read no H of the interior box), so the
+// latency-bound shell fills the bandwidth the interior kernel leaves.  Joined
+// back to the caller's stream by an event before the rim E cells.
 struct SideStream {
     cudaStream_t s = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -735,10 +744,10 @@ void profile_enable(bool on) {
     g_prof.on = on;
 }
 
-cudaError_t profile_read(double ms[4], int *steps) {
+cudaError_t profile_read(double ms[5], int *steps) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     cudaError_t e = prof_flush_locked();
-    for (int s = 0; s < 4; ++s) ms[s] = g_prof.ms[s];
+    for (int s = 0; s < NPROF; ++s) ms[s] = g_prof.ms[s];
     *steps = g_prof.steps;
     return e;
 }
@@ -760,48 +769,60 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
     }
     FusedMaps maps;
     if (use_interior && !build_maps<T>(a, maps)) use_interior = false;
-    ShellBox hbox, ebox;
+    // hbox = B (H of the interior kernel), ebox = B' (its E), rbox = [lo, hi+1):
+    // the E cells outside rbox read no H of B, the rim rbox \ B' does
+    ShellBox hbox, ebox, rbox, none, all;
     for (int d = 0; d < 3; ++d) {
+        all.lo[d] = 0;
+        all.hi[d] = n[d];
         hbox.lo[d] = use_interior ? a.npml : 0;
         hbox.hi[d] = use_interior ? n[d] - a.npml : 0;
         ebox.lo[d] = use_interior ? a.npml + 1 : 0;
         ebox.hi[d] = use_interior ? n[d] - a.npml : 0;
+        rbox.lo[d] = use_interior ? a.npml : 0;
+        rbox.hi[d] = use_interior ? n[d] - a.npml + 1 : n[d];
+        none.lo[d] = none.hi[d] = 0;
     }
     SideStream *side = nullptr;
     if (use_interior) {
         cudaError_t e = side_stream(&side);
         if (e != cudaSuccess) return e;
     }
-    std::array<cudaEvent_t, 6> ev;
+    std::array<cudaEvent_t, NEV> ev;
     const bool prof = prof_begin(ev);
     if (prof) cudaEventRecord(ev[0], st);
     cudaError_t e = cudaSuccess;
     if (use_interior) {
-        // shell H on the side stream, concurrent with the interior kernel
+        // shell H, then the outer shell E, on the side stream, concurrent with
+        // the interior kernel
         if ((e = cudaEventRecord(side->fork, st)) == cudaSuccess &&
             (e = cudaStreamWaitEvent(side->s, side->fork, 0)) == cudaSuccess)
             e = launch_shell_H<T>(a, hbox, side->s);
         if (prof) cudaEventRecord(ev[1], side->s);
+        if (e == cudaSuccess) e = launch_shell_E_region<T>(a, all, rbox, src, pl, side->s);
+        if (prof) cudaEventRecord(ev[2], side->s);
         cudaError_t e2 = cudaEventRecord(side->join, side->s);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = launch_interior<T>(a, maps, hbox, src, st);
-        if (prof) cudaEventRecord(ev[2], st);
+        if (prof) cudaEventRecord(ev[3], st);
         e2 = cudaStreamWaitEvent(st, side->join, 0);
         if (e == cudaSuccess) e = e2;
     } else {
-        e = launch_shell_H<T>(a, hbox, st);
+        e = launch_shell_H<T>(a, none, st);
         if (prof) {
             cudaEventRecord(ev[1], st);
             cudaEventRecord(ev[2], st);
+            cudaEventRecord(ev[3], st);
         }
     }
-    if (prof) cudaEventRecord(ev[3], st);
+    if (prof) cudaEventRecord(ev[4], st);
     // plane DFTs of the cells the interior kernel updated
     if (e == cudaSuccess && use_interior && pl.n) e = launch_plane_dft_box<T>(a, ebox, pl, st);
-    if (prof) cudaEventRecord(ev[4], st);
-    if (e == cudaSuccess) e = launch_shell_E<T>(a, ebox, src, pl, st);
+    if (prof) cudaEventRecord(ev[5], st);
+    // E of the rim (or of the whole grid without an interior box)
+    if (e == cudaSuccess) e = launch_shell_E_region<T>(a, rbox, ebox, src, pl, st);
     if (prof) {
-        cudaEventRecord(ev[5], st);
+        cudaEventRecord(ev[6], st);
         prof_end(ev);
     }
     return e;

@@ -35,6 +35,10 @@ cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t 
 template <typename T>
 cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceList &src,
                            const PlaneList &pl, cudaStream_t st);
+// E^{n+1} of the cells of box o outside box b (b empty: all of o).
+template <typename T>
+cudaError_t launch_shell_E_region(const YeeArgs<T> &a, const ShellBox &o, const ShellBox &b,
+                                  const SourceList &src, const PlaneList &pl, cudaStream_t st);
 
 // Plane-DFT accumulation for the monitored planes' cells inside box b (read
 // back from E_next / H_next after the interior update).

@@ -3,21 +3,25 @@
 // The fused step splits the grid into the interior box handled by the
 // single-pass kernel (yee_fused.cu) and a shell around it handled here, one
 // thread per cell:
-//   k_shell_H : H^{n+1/2} of every cell outside the box [lo, hi)^3 (the CPML
-//               slabs; the whole grid when there is no box), H read from H and
-//               written to H_next, psi_H in place.  Runs first.
-//   k_shell_E : E^{n+1} of every cell outside [lo+1, hi)^3 (the slabs plus the
-//               first interior layer, whose H neighbours straddle the slab
-//               boundary), reading the final H^{n+1/2} from H_next, writing
-//               E_next, psi_E in place, with the sheet injections and plane
-//               DFTs of those cells.  Runs after the interior kernel.
+//   k_shell_H : H^{n+1/2} of every cell outside the box B = [lo, hi)^3 (the
+//               CPML slabs; the whole grid when there is no box), H read from H
+//               and written to H_next, psi_H in place.
+//   k_shell_E : E^{n+1} of the cells of an outer box that lie outside an inner
+//               box, reading H^{n+1/2} from H_next, writing E_next, psi_E in
+//               place, with the sheet injections and plane DFTs of those cells.
+//               The fused step launches it twice: for the cells outside
+//               [lo, hi+1)^3, whose stencils read no H of B (right after
+//               k_shell_H, concurrent with the interior kernel), and for the
+//               one-cell rim [lo, hi+1)^3 minus [lo+1, hi)^3, whose stencils do
+//               (after the interior kernel).
 // Per-cell arithmetic is yee_cell.cuh (reference yee_update.cl), so each cell
 // rounds exactly as in the split kernels.
 //
-// Shell enumeration: a flat cell index over three disjoint groups,
-//   A: i outside [lo_x, hi_x)                      all (j, k)
-//   B: i inside,  j outside [lo_y, hi_y)           all k
-//   C: i inside,  j inside,  k outside [lo_z, hi_z)
+// Shell enumeration: a flat cell index over three disjoint groups of the outer
+// box o minus the inner box b,
+//   A: i in o, outside b                          all (j, k) of o
+//   B: i in b, j in o outside b                   all k of o
+//   C: i in b, j in b, k in o outside b
 // decoded with multiply-high divisions (consecutive threads take consecutive k).
 #include <cuda_runtime.h>
 
@@ -48,25 +52,29 @@ __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) {
     return (unsigned)(((unsigned long long)__umulhi(n, f.m) + n) >> f.l);
 }
 
-// Host-precomputed sizes of the three groups and their divisors.
+// Host-precomputed sizes of the three groups and their divisors.  The cells
+// enumerated are those of the outer box o = [o.lo, o.hi) that lie outside the
+// inner box b = [b.lo, b.hi) (b inside o; lo == hi on every axis means an empty
+// inner box, so the whole outer box is enumerated).
 struct ShellPlan {
-    ShellBox b;
-    int nax, nay, bx, by, cpr;  // slab planes in x, slab rows in y, box extents, C cells/row
-    unsigned nA, nB, nC;        // cells per group
-    FastDiv d_plane, d_nz, d_slab, d_cpr, d_by;  // ny*nz, nz, nay*nz, cpr, by
+    ShellBox b, o;
+    int nax, nay, bx, by, cpr, oy, oz;  // slab planes in x, slab rows in y, inner extents,
+                                        // C cells per row, outer extents in y and z
+    unsigned nA, nB, nC;                // cells per group
+    FastDiv d_plane, d_nz, d_slab, d_cpr, d_by;  // oy*oz, oz, nay*oz, cpr, by
 };
 
-__device__ __forceinline__ bool shell_cell(unsigned t, int nx, int ny, int nz,
-                                           const ShellPlan &s, int &i, int &j, int &k) {
-    (void)nx;
-    (void)ny;
+__device__ __forceinline__ bool shell_cell(unsigned t, const ShellPlan &s, int &i, int &j,
+                                           int &k) {
+    const unsigned oz = (unsigned)s.oz;
     if (t < s.nA) {
         const unsigned q = fdiv(t, s.d_plane);
         const unsigned rem = t - q * s.d_plane.d;
-        i = (int)q < s.b.lo[0] ? (int)q : s.b.hi[0] + ((int)q - s.b.lo[0]);
+        const int nlo = s.b.lo[0] - s.o.lo[0];
+        i = (int)q < nlo ? s.o.lo[0] + (int)q : s.b.hi[0] + ((int)q - nlo);
         const unsigned jj = fdiv(rem, s.d_nz);
-        j = (int)jj;
-        k = (int)(rem - jj * (unsigned)nz);
+        j = s.o.lo[1] + (int)jj;
+        k = s.o.lo[2] + (int)(rem - jj * oz);
         return true;
     }
     t -= s.nA;
@@ -75,8 +83,9 @@ __device__ __forceinline__ bool shell_cell(unsigned t, int nx, int ny, int nz,
         const unsigned rem = t - q * s.d_slab.d;
         i = s.b.lo[0] + (int)q;
         const unsigned r = fdiv(rem, s.d_nz);
-        j = (int)r < s.b.lo[1] ? (int)r : s.b.hi[1] + ((int)r - s.b.lo[1]);
-        k = (int)(rem - r * (unsigned)nz);
+        const int nlo = s.b.lo[1] - s.o.lo[1];
+        j = (int)r < nlo ? s.o.lo[1] + (int)r : s.b.hi[1] + ((int)r - nlo);
+        k = s.o.lo[2] + (int)(rem - r * oz);
         return true;
     }
     t -= s.nB;
@@ -86,26 +95,34 @@ __device__ __forceinline__ bool shell_cell(unsigned t, int nx, int ny, int nz,
         const unsigned bi = fdiv(row, s.d_by);
         i = s.b.lo[0] + (int)bi;
         j = s.b.lo[1] + (int)(row - bi * (unsigned)s.by);
-        k = c < s.b.lo[2] ? c : s.b.hi[2] + (c - s.b.lo[2]);
+        const int nlo = s.b.lo[2] - s.o.lo[2];
+        k = c < nlo ? s.o.lo[2] + c : s.b.hi[2] + (c - nlo);
         return true;
     }
     return false;
 }
 
-ShellPlan make_plan(int nx, int ny, int nz, const ShellBox &b) {
+// An empty inner box (lo == hi == 0 on every axis) enumerates all of o.
+ShellPlan make_plan(const ShellBox &o, const ShellBox &b) {
     ShellPlan s;
+    s.o = o;
     s.b = b;
-    s.nax = b.lo[0] + (nx - b.hi[0]);
-    s.nay = b.lo[1] + (ny - b.hi[1]);
-    s.bx = b.hi[0] - b.lo[0];
-    s.by = b.hi[1] - b.lo[1];
-    s.cpr = b.lo[2] + (nz - b.hi[2]);
-    s.nA = (unsigned)((int64_t)s.nax * ny * nz);
-    s.nB = (unsigned)((int64_t)s.bx * s.nay * nz);
+    if (b.lo[0] == b.hi[0] && b.lo[1] == b.hi[1] && b.lo[2] == b.hi[2])
+        for (int d = 0; d < 3; ++d) s.b.lo[d] = s.b.hi[d] = o.lo[d];
+    const ShellBox &B = s.b;
+    s.oy = o.hi[1] - o.lo[1];
+    s.oz = o.hi[2] - o.lo[2];
+    s.nax = (B.lo[0] - o.lo[0]) + (o.hi[0] - B.hi[0]);
+    s.nay = (B.lo[1] - o.lo[1]) + (o.hi[1] - B.hi[1]);
+    s.bx = B.hi[0] - B.lo[0];
+    s.by = B.hi[1] - B.lo[1];
+    s.cpr = (B.lo[2] - o.lo[2]) + (o.hi[2] - B.hi[2]);
+    s.nA = (unsigned)((int64_t)s.nax * s.oy * s.oz);
+    s.nB = (unsigned)((int64_t)s.bx * s.nay * s.oz);
     s.nC = (unsigned)((int64_t)s.bx * s.by * s.cpr);
-    s.d_plane = make_fastdiv((unsigned)ny * (unsigned)nz);
-    s.d_nz = make_fastdiv((unsigned)nz);
-    s.d_slab = make_fastdiv((unsigned)s.nay * (unsigned)nz);
+    s.d_plane = make_fastdiv((unsigned)s.oy * (unsigned)s.oz);
+    s.d_nz = make_fastdiv((unsigned)s.oz);
+    s.d_slab = make_fastdiv((unsigned)s.nay * (unsigned)s.oz);
     s.d_cpr = make_fastdiv((unsigned)(s.cpr > 0 ? s.cpr : 0));
     s.d_by = make_fastdiv((unsigned)(s.by > 0 ? s.by : 0));
     return s;
@@ -118,7 +135,7 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     k_shell_H(YeeArgs<T> a, ShellPlan sp) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, npml = a.npml;
     int i, j, k;
-    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, nx, ny, nz, sp, i, j, k)) return;
+    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Ex = a.E[0], *Ey = a.E[1], *Ez = a.E[2];
@@ -153,7 +170,7 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     k_shell_E(YeeArgs<T> a, ShellPlan sp, SourceList src, const __grid_constant__ PlaneList planes) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, npml = a.npml;
     int i, j, k;
-    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, nx, ny, nz, sp, i, j, k)) return;
+    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Hx = a.H_next[0], *Hy = a.H_next[1], *Hz = a.H_next[2];
@@ -238,19 +255,26 @@ static unsigned shell_blocks(const ShellPlan &s) {
     return (unsigned)((n + SHELL_THREADS - 1) / SHELL_THREADS);
 }
 
-static bool plan_fits(int nx, int ny, int nz, const ShellBox &b) {
+static bool plan_fits(const ShellBox &o) {
     // every group count and the flat index must fit in 32 bits
-    const int64_t nax = b.lo[0] + (nx - b.hi[0]), nay = b.lo[1] + (ny - b.hi[1]);
-    const int64_t tot = nax * ny * nz + (int64_t)(b.hi[0] - b.lo[0]) * nay * nz +
-                        (int64_t)(b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) *
-                            (b.lo[2] + (nz - b.hi[2]));
-    return tot + SHELL_THREADS < 0xffffffffLL && (int64_t)ny * nz < 0xffffffffLL;
+    const int64_t ex[3] = {o.hi[0] - o.lo[0], o.hi[1] - o.lo[1], o.hi[2] - o.lo[2]};
+    return ex[0] * ex[1] * ex[2] + SHELL_THREADS < 0xffffffffLL;
+}
+
+static ShellBox whole_grid(int nx, int ny, int nz) {
+    ShellBox o;
+    o.lo[0] = o.lo[1] = o.lo[2] = 0;
+    o.hi[0] = nx;
+    o.hi[1] = ny;
+    o.hi[2] = nz;
+    return o;
 }
 
 template <typename T>
 cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t st) {
-    if (!plan_fits(a.nx, a.ny, a.nz, b)) return cudaErrorInvalidConfiguration;
-    const ShellPlan sp = make_plan(a.nx, a.ny, a.nz, b);
+    const ShellBox o = whole_grid(a.nx, a.ny, a.nz);
+    if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
+    const ShellPlan sp = make_plan(o, b);
     const unsigned nb = shell_blocks(sp);
     if (nb == 0) return cudaSuccess;
     k_shell_H<T><<<nb, SHELL_THREADS, 0, st>>>(a, sp);
@@ -259,10 +283,10 @@ cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t 
 }
 
 template <typename T>
-cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceList &src,
-                           const PlaneList &pl, cudaStream_t st) {
-    if (!plan_fits(a.nx, a.ny, a.nz, b)) return cudaErrorInvalidConfiguration;
-    const ShellPlan sp = make_plan(a.nx, a.ny, a.nz, b);
+cudaError_t launch_shell_E_region(const YeeArgs<T> &a, const ShellBox &o, const ShellBox &b,
+                                  const SourceList &src, const PlaneList &pl, cudaStream_t st) {
+    if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
+    const ShellPlan sp = make_plan(o, b);
     const unsigned nb = shell_blocks(sp);
     if (nb == 0) return cudaSuccess;
     if (a.lossy)
@@ -273,6 +297,18 @@ cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceL
     return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceList &src,
+                           const PlaneList &pl, cudaStream_t st) {
+    return launch_shell_E_region<T>(a, whole_grid(a.nx, a.ny, a.nz), b, src, pl, st);
+}
+
+template cudaError_t launch_shell_E_region<float>(const YeeArgs<float> &, const ShellBox &,
+                                                  const ShellBox &, const SourceList &,
+                                                  const PlaneList &, cudaStream_t);
+template cudaError_t launch_shell_E_region<double>(const YeeArgs<double> &, const ShellBox &,
+                                                   const ShellBox &, const SourceList &,
+                                                   const PlaneList &, cudaStream_t);
 template cudaError_t launch_shell_H<float>(const YeeArgs<float> &, const ShellBox &, cudaStream_t);
 template cudaError_t launch_shell_H<double>(const YeeArgs<double> &, const ShellBox &,
                                             cudaStream_t);

@@ -507,13 +507,13 @@ def test_launch_counter_and_step_profile(cuda):
     capi.run("fdtd_profile_steps", 1)
     g.run(5)
     capi.run("fdtd_profile_steps", 0)
-    ms = (ctypes.c_double * 4)()
+    ms = (ctypes.c_double * 5)()
     n = ctypes.c_int32()
     capi.run("fdtd_profile_read", ms, ctypes.byref(n))
     assert n.value == 5
     assert all(v > 0 for v in ms)
-    # shell H, interior, plane DFT of the interior, shell E per step
-    assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
+    # shell H, outer shell E, interior, plane DFT of the interior, rim E per step
+    assert capi.lib().fdtd_launch_count() - n0 == 5 * 5
 
 
 @pytest.mark.parametrize("steps", [200, 2000], ids=["200_steps", "full_2000_steps"])
