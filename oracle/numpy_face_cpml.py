@@ -21,7 +21,10 @@ fields equal the reference engine's bit for bit (pinned by
 ``tests/test_numpy_port.py`` against ``tests/golden/numpy_ref.npz``, which was
 made by importing the reference).  ``courant=`` reproduces the reference
 override used for the configurations quoted at Courant 0.5 (set ``dt``, rebuild
-``ce`` and the CPML profiles).
+``ce`` and the CPML profiles).  ``slab=`` (an ``opencl_fdtd_solver_b200.slabs.SlabLocal``)
+runs one x-slab of a larger grid: the local planes with their ghosts, the x-CPML
+only on global faces, the global profiles' slice, and sheets given in global
+indices; the multi-rank CPU tests hold such slabs to the single-domain run.
 
 Only tests and ``bench.py``'s CPU-baseline legs use this module, as the checker
 and as the timed NumPy baseline; the product never imports it.
@@ -74,8 +77,14 @@ def _bcast(v, axis):
 class NumPyFaceCPML:
     """CPU FDTD with the reference's NumPy face-CPML arithmetic."""
 
-    def __init__(self, shape, dl, npml=20, dtype=np.float32, courant=None):
-        self.Nx, self.Ny, self.Nz = (int(v) for v in shape)
+    def __init__(self, shape, dl, npml=20, dtype=np.float32, courant=None, slab=None):
+        self.slab = slab
+        self.global_shape = tuple(int(v) for v in shape)
+        self.Nx, self.Ny, self.Nz = self.global_shape
+        # x-planes of the local grid: global [x0, x0 + Nx); CPML layers per x side
+        self.x0, self.pml_x = 0, (int(npml), int(npml))
+        if slab is not None:
+            self.Nx, self.x0, self.pml_x = slab.nx_local, slab.l0, (slab.pml_lo, slab.pml_hi)
         self.shape = (self.Nx, self.Ny, self.Nz)
         self.dl = float(dl)
         self.npml = int(npml)
@@ -86,30 +95,43 @@ class NumPyFaceCPML:
                    else float(courant) * self.dl / hm.C0)
         for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
             setattr(self, n, np.zeros(self.shape, self.dtype))
-        self.set_epsilon(np.ones(self.shape, self.dtype))
+        self.set_epsilon(np.ones(self.global_shape, self.dtype))
         self._sources = []
         self._monitors = []
         self._build_cpml()
 
     # ------------------------------------------------------------ set-up
     def set_epsilon(self, eps):
-        if eps.shape != self.shape:
-            raise ValueError(f"Epsilon shape mismatch: expected {self.shape}, got {eps.shape}")
-        eps_r = eps.astype(self.dtype)
+        """εr of the whole grid (``global_shape``); a slab takes its planes."""
+        if eps.shape != self.global_shape:
+            raise ValueError(f"Epsilon shape mismatch: expected {self.global_shape}, "
+                             f"got {eps.shape}")
+        eps_r = eps[self.x0:self.x0 + self.Nx].astype(self.dtype)
         self.ce = list(hm.edge_ce(eps_r, self.dt, self.dtype))
 
+    def _sides(self, axis):
+        """CPML layers (low, high) along ``axis`` on the local grid."""
+        return self.pml_x if axis == 0 else (self.npml, self.npml)
+
     def _build_cpml(self):
-        prof = hm.cpml_all(self.shape, self.npml, self.dl, self.dt, self.dtype)
+        prof = hm.cpml_all(self.global_shape, self.npml, self.dl, self.dt, self.dtype)
+        sel = slice(self.x0, self.x0 + self.Nx)  # the local planes of the x profiles
         # per stagger and axis: b, c on the axis and κ broadcast for the volume curls
-        self._prof = {s: [(b, c, _bcast(kap, a)) for a, (b, c, _ik, kap) in enumerate(prof[s])]
-                      for s in ("h", "e")}
-        n = self.npml
+        self._prof = {}
+        for st in ("h", "e"):
+            axes = []
+            for a, (b, c, _ik, kap) in enumerate(prof[st]):
+                if a == 0:
+                    b, c, kap = b[sel], c[sel], kap[sel]
+                axes.append((b, c, _bcast(kap, a)))
+            self._prof[st] = axes
         self._psi = {}
         for a in range(3):
+            lo, hi = self._sides(a)
             shp = list(self.shape)
-            shp[a] = 2 * n
+            shp[a] = lo + hi
             for name, _d, _s in _H_TERMS[a] + _E_TERMS[a]:
-                self._psi[(name, a)] = np.zeros(shp if n > 0 else (0,), self.dtype)
+                self._psi[(name, a)] = np.zeros(shp if self.npml > 0 else (0,), self.dtype)
 
     def add_source(self, cb):
         if not callable(cb):
@@ -125,12 +147,22 @@ class NumPyFaceCPML:
 
     # ------------------------------------------------------------ sources
     def _span(self, i0, i1, j0, j1):
-        return (0 if i0 is None else int(i0), self.Nx if i1 is None else int(i1),
+        """Sheet bounds in global indices (defaults: the whole global plane)."""
+        return (0 if i0 is None else int(i0), self.global_shape[0] if i1 is None else int(i1),
                 0 if j0 is None else int(j0), self.Ny if j1 is None else int(j1))
+
+    def _local_rows(self, a0, a1):
+        """The sheet rows [a0, a1) (global) that lie on the local grid: the local
+        slice and the matching slice of the sheet's own row index."""
+        l0, l1 = max(a0, self.x0), min(a1, self.x0 + self.Nx)
+        if l1 <= l0:
+            return slice(0, 0), slice(0, 0)
+        return slice(l0 - self.x0, l1 - self.x0), slice(l0 - a0, l1 - a0)
 
     def add_source_Ex(self, z_src, amp, i0=None, i1=None, j0=None, j1=None):
         a0, a1, b0, b1 = self._span(i0, i1, j0, j1)
-        self.Ex[a0:a1, b0:b1, int(z_src)] += self.dtype.type(amp)
+        loc, _ = self._local_rows(a0, a1)
+        self.Ex[loc, b0:b1, int(z_src)] += self.dtype.type(amp)
 
     def add_source_Jx(self, z_src, Jx, i0=None, i1=None, j0=None, j1=None, *,
                       rim_taper=False, rim_edge=0.8, rim_renorm=True):
@@ -141,7 +173,8 @@ class NumPyFaceCPML:
             inner_a, inner_b = na - 2, nb - 2
             total = inner_a * inner_b + re * (2 * inner_a + 2 * inner_b) + (re * re) * 4
             jx *= (na * nb) / total
-        inj = -self.ce[0][a0:a1, b0:b1, z] * jx
+        loc, rows = self._local_rows(a0, a1)
+        inj = -self.ce[0][loc, b0:b1, z] * jx
         if rim_taper:
             w = np.ones((na, nb), self.dtype)
             if na >= 1:
@@ -150,14 +183,20 @@ class NumPyFaceCPML:
             if nb >= 1:
                 w[:, 0] *= re
                 w[:, -1] *= re
-            inj = inj * w
-        self.Ex[a0:a1, b0:b1, z] += inj.astype(self.dtype, copy=False)
+            inj = inj * w[rows]
+        self.Ex[loc, b0:b1, z] += inj.astype(self.dtype, copy=False)
 
     # ------------------------------------------------------------ update
     def _faces(self, axis):
         """(domain slice, stripe slice) of the low then the high stripe."""
-        n, p = self.shape[axis], self.npml
-        return ((slice(0, p), slice(0, p)), (slice(n - p, n), slice(p, 2 * p)))
+        n = self.shape[axis]
+        lo, hi = self._sides(axis)
+        out = []
+        if lo > 0:
+            out.append((slice(0, lo), slice(0, lo)))
+        if hi > 0:
+            out.append((slice(n - hi, n), slice(lo, lo + hi)))
+        return out
 
     def _stripe_terms(self, terms, stag, diffs, apply):
         for a in range(3):
