@@ -50,6 +50,16 @@ typedef struct {
     int32_t dtype;          /* FDTD_F32 or FDTD_F64                            */
     int32_t lossy;          /* nonzero: E = ca*E + ...; zero: ca == 1, not read */
     double dtm, dtm_dl, inv_dl;
+    /* x-slab of a grid decomposed along x (x_slab == 0: the whole grid, npml
+     * CPML layers on both x faces; the remaining fields are then ignored).
+     * x_slab != 0: this grid is one slab; pml_x_lo / pml_x_hi are its x-CPML
+     * layers (npml on a global face, else 0), ghost_lo / ghost_hi (0 or 1) mark
+     * a ghost plane at local x = 0 / nx-1 that holds a neighbour's plane.  Ghost
+     * planes are advanced with boundary-guarded differences and are to be
+     * overwritten by the caller's exchange; the x CPML profiles and psi_x stripes
+     * ((pml_x_lo + pml_x_hi) x ny x nz) are the slab's own.  No reference
+     * counterpart (the reference runs one device). */
+    int32_t x_slab, pml_x_lo, pml_x_hi, ghost_lo, ghost_hi, pad_;
 } fdtd_grid;
 
 /* Field state.  E/H hold the state at step n (E^n, H^{n-1/2}).

@@ -42,7 +42,9 @@ V6 = c_void_p * 6
 class Grid(Structure):
     _fields_ = [("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("npml", c_int32),
                 ("dtype", c_int32), ("lossy", c_int32),
-                ("dtm", c_double), ("dtm_dl", c_double), ("inv_dl", c_double)]
+                ("dtm", c_double), ("dtm_dl", c_double), ("inv_dl", c_double),
+                ("x_slab", c_int32), ("pml_x_lo", c_int32), ("pml_x_hi", c_int32),
+                ("ghost_lo", c_int32), ("ghost_hi", c_int32), ("pad_", c_int32)]
 
 
 class Fields(Structure):

@@ -79,7 +79,41 @@ int check_grid(const fdtd_grid *g) {
     if (g->npml < 0) return fail(FDTD_ERR_INVALID, "npml must be >= 0, got %d", g->npml);
     if (g->dtype != FDTD_F32 && g->dtype != FDTD_F64)
         return fail(FDTD_ERR_INVALID, "dtype must be FDTD_F32 or FDTD_F64, got %d", g->dtype);
+    if (g->x_slab) {
+        if ((g->pml_x_lo != 0 && g->pml_x_lo != g->npml) ||
+            (g->pml_x_hi != 0 && g->pml_x_hi != g->npml))
+            return fail(FDTD_ERR_INVALID, "slab x-CPML layers (%d, %d) must each be 0 or npml=%d",
+                        g->pml_x_lo, g->pml_x_hi, g->npml);
+        if ((g->ghost_lo != 0 && g->ghost_lo != 1) || (g->ghost_hi != 0 && g->ghost_hi != 1))
+            return fail(FDTD_ERR_INVALID, "slab ghost flags (%d, %d) must be 0 or 1", g->ghost_lo,
+                        g->ghost_hi);
+        if ((g->ghost_lo && g->pml_x_lo) || (g->ghost_hi && g->pml_x_hi))
+            return fail(FDTD_ERR_INVALID, "a slab face is either a ghost or an x-CPML face");
+        if (g->npml < 1)
+            return fail(FDTD_ERR_INVALID, "a slab needs npml >= 1");
+        if (g->nx < g->pml_x_lo + g->pml_x_hi + g->ghost_lo + g->ghost_hi + 1)
+            return fail(FDTD_ERR_INVALID, "slab of %d planes is thinner than its CPML and ghosts",
+                        g->nx);
+    }
     return FDTD_OK;
+}
+
+// x CPML layers and interior x bounds of a grid or slab.
+fdtd::XBounds x_bounds(const fdtd_grid *g) {
+    fdtd::XBounds xb;
+    if (g->x_slab) {
+        // H's interior form reads E at x+1 (not on the upper ghost), E's reads H
+        // at x-1 (not on the lower ghost)
+        xb.pml_lo = g->pml_x_lo;
+        xb.pml_hi = g->pml_x_hi;
+        xb.h_lo = g->pml_x_lo;
+        xb.h_hi = g->pml_x_hi > g->ghost_hi ? g->pml_x_hi : g->ghost_hi;
+        xb.e_lo = g->pml_x_lo > g->ghost_lo ? g->pml_x_lo : g->ghost_lo;
+        xb.e_hi = g->pml_x_hi;
+    } else {
+        xb.pml_lo = xb.pml_hi = xb.h_lo = xb.h_hi = xb.e_lo = xb.e_hi = g->npml;
+    }
+    return xb;
 }
 
 int check_fields(const fdtd_grid *g, const fdtd_fields *f, bool need_next) {
@@ -161,6 +195,9 @@ fdtd::YeeArgs<T> make_args(const fdtd_grid *g, const fdtd_fields *f, const fdtd_
     a.nz = g->nz;
     a.npml = g->npml;
     a.lossy = g->lossy ? 1 : 0;
+    a.xb = x_bounds(g);
+    a.ghost_lo = g->x_slab ? g->ghost_lo : 0;
+    a.ghost_hi = g->x_slab ? g->ghost_hi : 0;
     a.dtm = (T)g->dtm;
     a.dtm_dl = (T)g->dtm_dl;
     a.inv_dl = (T)g->inv_dl;
@@ -212,6 +249,8 @@ int check_box(const fdtd_grid *g, const fdtd_box *b) {
 // ---- adjoint --------------------------------------------------------------
 int check_adjoint(const fdtd_grid *g, const fdtd_adjoint_fields *a) {
     if (!a) return fail(FDTD_ERR_INVALID, "adjoint fields is NULL");
+    if (g->x_slab)
+        return fail(FDTD_ERR_UNSUPPORTED, "the adjoint sweep runs on a whole grid, not a slab");
     if (g->lossy)
         return fail(FDTD_ERR_UNSUPPORTED, "the adjoint sweep needs a lossless grid (ca == 1)");
     for (int c = 0; c < 3; ++c)

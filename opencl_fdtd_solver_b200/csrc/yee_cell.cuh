@@ -22,25 +22,52 @@ struct Cpml1D {
 };
 
 // ψ stripe offsets for one cell.  Layer l of axis a: low face l in [0,npml),
-// high face npml + (x - (N - npml)) (yee_update.cl:91,99,107).
+// high face npml + (x - (N - npml)) (yee_update.cl:91,99,107).  The x axis of
+// a slab of an x-decomposed grid has lo low and hi high layers (npml on a
+// global face, 0 on a face towards another slab); y and z have npml on both.
+__device__ __forceinline__ int pml_layer(int x, int n, int lo, int hi) {
+    return (x < lo) ? x : (lo + x - (n - hi));
+}
 __device__ __forceinline__ int pml_layer(int x, int n, int npml) {
-    return (x < npml) ? x : (npml + x - (n - npml));
+    return pml_layer(x, n, npml, npml);
 }
 
+__device__ __forceinline__ bool in_slab(int x, int n, int lo, int hi) {
+    return x < lo || x >= n - hi;
+}
 __device__ __forceinline__ bool in_slab(int x, int n, int npml) {
     return npml > 0 && (x < npml || x >= n - npml);
 }
 
+// The x range [xlo, nx - xhi) of interior cells: the x CPML layers are
+// excluded and, on a slab, the ghost plane whose interior update would read
+// past the slab (the upper ghost for H, the lower for E), which takes the
+// boundary-guarded form instead.
+__device__ __forceinline__ bool is_interior(int i, int j, int k, int nx, int ny, int nz,
+                                            int npml, int xlo, int xhi) {
+    return npml > 0 && i >= xlo && i < nx - xhi && j >= npml && j < ny - npml &&
+           k >= npml && k < nz - npml;
+}
 __device__ __forceinline__ bool is_interior(int i, int j, int k, int nx, int ny, int nz,
                                             int npml) {
-    return npml > 0 && i >= npml && i < nx - npml && j >= npml && j < ny - npml &&
-           k >= npml && k < nz - npml;
+    return is_interior(i, j, k, nx, ny, nz, npml, npml, npml);
 }
 
 __device__ __forceinline__ int64_t psi_x_index(int i, int j, int k, int nx, int ny, int nz,
-                                               int npml) {
-    return ((int64_t)pml_layer(i, nx, npml) * ny + j) * nz + k;
+                                               int lo, int hi) {
+    return ((int64_t)pml_layer(i, nx, lo, hi) * ny + j) * nz + k;
 }
+__device__ __forceinline__ int64_t psi_x_index(int i, int j, int k, int nx, int ny, int nz,
+                                               int npml) {
+    return psi_x_index(i, j, k, nx, ny, nz, npml, npml);
+}
+
+// x-CPML layers of a Yee kernel's grid: (lo, hi), and the interior x bounds.
+struct XBounds {
+    int pml_lo, pml_hi;  // x CPML layers at the low / high x face
+    int h_lo, h_hi;      // interior H cells: x in [h_lo, nx - h_hi)
+    int e_lo, e_hi;      // interior E cells: x in [e_lo, nx - e_hi)
+};
 __device__ __forceinline__ int64_t psi_y_index(int i, int j, int k, int ny, int nz, int npml) {
     return ((int64_t)i * (2 * npml) + pml_layer(j, ny, npml)) * nz + k;
 }
@@ -60,7 +87,8 @@ struct DE {
 // in-place split kernel.  Returns the new H through hx/hy/hz.
 template <typename T, bool WRITE_PSI = true>
 __device__ __forceinline__ void h_cell(bool interior, int i, int j, int k, int nx, int ny,
-                                       int nz, int npml, T dtm, T dtm_dl, const DE<T> &d,
+                                       int nz, int npml, const XBounds &xb, T dtm, T dtm_dl,
+                                       const DE<T> &d,
                                        const Cpml1D<T> &cp, T *const *psi_rd, T *const *psi_wr,
                                        T &hx, T &hy, T &hz) {
     if (interior) {
@@ -71,8 +99,8 @@ __device__ __forceinline__ void h_cell(bool interior, int i, int j, int k, int n
     }
     // psi order: 0 Hx_y, 1 Hx_z, 2 Hy_x, 3 Hy_z, 4 Hz_x, 5 Hz_y
     T p_hx_y = T(0), p_hx_z = T(0), p_hy_x = T(0), p_hy_z = T(0), p_hz_x = T(0), p_hz_y = T(0);
-    if (in_slab(i, nx, npml)) {
-        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, npml);
+    if (npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi)) {
+        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi);
         const T b = cp.b[0][i], c = cp.c[0][i];
         p_hy_x = b * psi_rd[2][s] + c * d.zx;
         p_hz_x = b * psi_rd[4][s] + c * d.yx;
@@ -117,7 +145,8 @@ struct DH {
 // already added) and leave as E^{n+1}.  psi_e is updated in place.
 template <typename T, bool LOSSY>
 __device__ __forceinline__ void e_cell(bool interior, int i, int j, int k, int nx, int ny,
-                                       int nz, int npml, T inv_dl, const DH<T> &d,
+                                       int nz, int npml, const XBounds &xb, T inv_dl,
+                                       const DH<T> &d,
                                        const Cpml1D<T> &cp, T *const *psi_e, T cax, T cay,
                                        T caz, T cex, T cey, T cez, T &ex, T &ey, T &ez) {
     if (interior) {
@@ -128,8 +157,8 @@ __device__ __forceinline__ void e_cell(bool interior, int i, int j, int k, int n
     }
     // psi order: 0 Ex_y, 1 Ex_z, 2 Ey_x, 3 Ey_z, 4 Ez_x, 5 Ez_y
     T p_ex_y = T(0), p_ex_z = T(0), p_ey_x = T(0), p_ey_z = T(0), p_ez_x = T(0), p_ez_y = T(0);
-    if (in_slab(i, nx, npml)) {
-        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, npml);
+    if (npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi)) {
+        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi);
         const T b = cp.b[0][i], c = cp.c[0][i];
         p_ey_x = b * psi_e[2][s] + c * d.zx;
         p_ez_x = b * psi_e[4][s] + c * d.yx;

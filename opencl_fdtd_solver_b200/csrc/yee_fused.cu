@@ -757,10 +757,20 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
                               cudaStream_t st) {
     const int elem = (int)sizeof(T);
     const int n[3] = {a.nx, a.ny, a.nz};
-    // interior H box [npml, N-npml)^3; the fused kernel needs npml >= 1, a non
-    // empty E box and TMA-compatible (16-byte) strides and base addresses
+    // interior H box B = [npml, N-npml)^3 (x on a slab: [pml_lo, nx - pml_hi -
+    // ghost_hi), so the upper ghost plane, whose forward differences would read
+    // past the slab, is left to the boundary-guarded shell kernel); the fused
+    // kernel needs npml >= 1, a box of at least two cells per axis and
+    // TMA-compatible (16-byte) strides and base addresses
+    int blo[3], bhi[3];
+    for (int d = 0; d < 3; ++d) {
+        blo[d] = a.npml;
+        bhi[d] = n[d] - a.npml;
+    }
+    blo[0] = a.xb.pml_lo;
+    bhi[0] = n[0] - a.xb.pml_hi - a.ghost_hi;
     bool use_interior = a.npml >= 1 && ((int64_t)a.nz * elem) % 16 == 0;
-    for (int d = 0; d < 3; ++d) use_interior = use_interior && n[d] - 2 * a.npml >= 2;
+    for (int d = 0; d < 3; ++d) use_interior = use_interior && bhi[d] - blo[d] >= 2;
     for (int c = 0; c < 3 && use_interior; ++c) {
         const void *ptrs[5] = {a.E[c], a.H[c], a.ce[c], a.E_next[c], a.H_next[c]};
         for (const void *q : ptrs)
@@ -775,12 +785,12 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
     for (int d = 0; d < 3; ++d) {
         all.lo[d] = 0;
         all.hi[d] = n[d];
-        hbox.lo[d] = use_interior ? a.npml : 0;
-        hbox.hi[d] = use_interior ? n[d] - a.npml : 0;
-        ebox.lo[d] = use_interior ? a.npml + 1 : 0;
-        ebox.hi[d] = use_interior ? n[d] - a.npml : 0;
-        rbox.lo[d] = use_interior ? a.npml : 0;
-        rbox.hi[d] = use_interior ? n[d] - a.npml + 1 : n[d];
+        hbox.lo[d] = use_interior ? blo[d] : 0;
+        hbox.hi[d] = use_interior ? bhi[d] : 0;
+        ebox.lo[d] = use_interior ? blo[d] + 1 : 0;
+        ebox.hi[d] = use_interior ? bhi[d] : 0;
+        rbox.lo[d] = use_interior ? blo[d] : 0;
+        rbox.hi[d] = use_interior ? bhi[d] + 1 : n[d];
         none.lo[d] = none.hi[d] = 0;
     }
     SideStream *side = nullptr;

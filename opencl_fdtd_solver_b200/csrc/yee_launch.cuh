@@ -12,6 +12,8 @@ namespace fdtd {
 template <typename T>
 struct YeeArgs {
     int nx, ny, nz, npml, lossy;
+    XBounds xb;        // x CPML layers per face and interior x bounds (slabs)
+    int ghost_lo, ghost_hi;  // ghost planes at x = 0 / nx-1 (slabs only)
     T dtm, dtm_dl, inv_dl;
     T *E[3];
     T *H[3];

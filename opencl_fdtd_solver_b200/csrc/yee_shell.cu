@@ -139,7 +139,8 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Ex = a.E[0], *Ey = a.E[1], *Ez = a.E[2];
-    const bool interior = is_interior(i, j, k, nx, ny, nz, npml);
+    const bool interior =
+        is_interior(i, j, k, nx, ny, nz, npml, a.xb.h_lo, a.xb.h_hi);
     const T ex0 = Ex[idx], ey0 = Ey[idx], ez0 = Ez[idx];
     DE<T> d;
     d.zy = (j < ny - 1) ? (Ez[idx + sy] - ez0) : T(0);
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     d.yx = (i < nx - 1) ? (Ey[idx + sx] - ey0) : T(0);
     d.xy = (j < ny - 1) ? (Ex[idx + sy] - ex0) : T(0);
     T hx = a.H[0][idx], hy = a.H[1][idx], hz = a.H[2][idx];
-    h_cell<T, true>(interior, i, j, k, nx, ny, nz, npml, a.dtm, a.dtm_dl, d, a.cph, a.psi_h,
+    h_cell<T, true>(interior, i, j, k, nx, ny, nz, npml, a.xb, a.dtm, a.dtm_dl, d, a.cph, a.psi_h,
                     a.psi_h, hx, hy, hz);
     a.H_next[0][idx] = hx;
     a.H_next[1][idx] = hy;
@@ -174,7 +175,8 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Hx = a.H_next[0], *Hy = a.H_next[1], *Hz = a.H_next[2];
-    const bool interior = is_interior(i, j, k, nx, ny, nz, npml);
+    const bool interior =
+        is_interior(i, j, k, nx, ny, nz, npml, a.xb.e_lo, a.xb.e_hi);
     const T hx0 = Hx[idx], hy0 = Hy[idx], hz0 = Hz[idx];
     DH<T> d;
     d.zy = (j > 0) ? (hz0 - Hz[idx - sy]) : T(0);
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     }
     T ex = a.E[0][idx], ey = a.E[1][idx], ez = a.E[2][idx];
     if (src.n) ex = apply_sources<T>(src, i, j, k, ex, cex);
-    e_cell<T, LOSSY>(interior, i, j, k, nx, ny, nz, npml, a.inv_dl, d, a.cpe, a.psi_e, cax, cay,
+    e_cell<T, LOSSY>(interior, i, j, k, nx, ny, nz, npml, a.xb, a.inv_dl, d, a.cpe, a.psi_e, cax, cay,
                      caz, cex, cey, cez, ex, ey, ez);
     a.E_next[0][idx] = ex;
     a.E_next[1][idx] = ey;

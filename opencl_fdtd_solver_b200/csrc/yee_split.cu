@@ -29,7 +29,8 @@ __global__ void __launch_bounds__(SPLIT_TK *SPLIT_TJ)
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Ex = a.E[0], *Ey = a.E[1], *Ez = a.E[2];
-    const bool interior = is_interior(i, j, k, nx, ny, nz, npml);
+    const bool interior =
+        is_interior(i, j, k, nx, ny, nz, npml, a.xb.h_lo, a.xb.h_hi);
     DE<T> d;
     const T ex0 = Ex[idx], ey0 = Ey[idx], ez0 = Ez[idx];
     if (interior) {
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(SPLIT_TK *SPLIT_TJ)
         d.xy = (j < ny - 1) ? (Ex[idx + sy] - ex0) : T(0);
     }
     T hx = a.H[0][idx], hy = a.H[1][idx], hz = a.H[2][idx];
-    h_cell<T>(interior, i, j, k, nx, ny, nz, npml, a.dtm, a.dtm_dl, d, a.cph, a.psi_h,
+    h_cell<T>(interior, i, j, k, nx, ny, nz, npml, a.xb, a.dtm, a.dtm_dl, d, a.cph, a.psi_h,
               a.psi_h, hx, hy, hz);
     a.H[0][idx] = hx;
     a.H[1][idx] = hy;
@@ -66,7 +67,8 @@ __global__ void __launch_bounds__(SPLIT_TK *SPLIT_TJ)
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Hx = a.H[0], *Hy = a.H[1], *Hz = a.H[2];
-    const bool interior = is_interior(i, j, k, nx, ny, nz, npml);
+    const bool interior =
+        is_interior(i, j, k, nx, ny, nz, npml, a.xb.e_lo, a.xb.e_hi);
     const T hx0 = Hx[idx], hy0 = Hy[idx], hz0 = Hz[idx];
     DH<T> d;
     if (interior) {
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(SPLIT_TK *SPLIT_TJ)
     }
     T ex = a.E[0][idx], ey = a.E[1][idx], ez = a.E[2][idx];
     if (src.n) ex = apply_sources<T>(src, i, j, k, ex, cex);
-    e_cell<T, LOSSY>(interior, i, j, k, nx, ny, nz, npml, a.inv_dl, d, a.cpe, a.psi_e, cax, cay,
+    e_cell<T, LOSSY>(interior, i, j, k, nx, ny, nz, npml, a.xb, a.inv_dl, d, a.cpe, a.psi_e, cax, cay,
                      caz, cex, cey, cez, ex, ey, ez);
     a.E[0][idx] = ex;
     a.E[1][idx] = ey;

@@ -60,7 +60,7 @@ class CUDAFDTD(SourceMonitorMixin):
     MEMORY_HEADROOM_BYTES = 512 * 1024 * 1024
 
     def __init__(self, shape, dl, npml=20, dtype=np.float32, ctx=None, queue=None,
-                 accum_fp64=False, *, courant=None, device=None, fused=True):
+                 accum_fp64=False, *, courant=None, device=None, fused=True, slab=None):
         """
         shape : (Nx, Ny, Nz) Yee cells
         dl    : uniform cell size in metres
@@ -75,8 +75,20 @@ class CUDAFDTD(SourceMonitorMixin):
             fixed 0.99/√3
         device : CUDA device (index, string or ``torch.device``); default current
         fused : run steps with the single-pass kernel when the shape allows it
+        slab  : a ``slabs.SlabLocal``: run one x-slab of the grid ``shape`` (its
+            planes plus ghost planes, ``Nx`` = the local plane count, the x-CPML
+            only on global faces).  ``set_epsilon`` then takes the whole grid's
+            εr and sheets take global i indices; field reads return the local
+            planes.  ``slabs.SlabFDTD`` drives one slab per rank.
         """
-        self.Nx, self.Ny, self.Nz = (int(v) for v in shape)
+        self.global_shape = tuple(int(v) for v in shape)
+        self.Nx, self.Ny, self.Nz = self.global_shape
+        self.slab = slab
+        self.x0 = 0  # global index of local plane 0
+        if slab is not None:
+            if slab.nx != self.Nx or slab.npml != int(npml):
+                raise ValueError(f"slab {slab} does not belong to shape {shape} / npml {npml}")
+            self.Nx, self.x0 = slab.nx_local, slab.l0
         self.dl = float(dl)
         self.npml = int(npml)
         dtype = np.dtype(dtype)
@@ -105,7 +117,8 @@ class CUDAFDTD(SourceMonitorMixin):
             self.dt = self.courant * self.dl / C0
         self.size = self.Nx * self.Ny * self.Nz
         n = self.npml
-        self.psi_x_size = 2 * n * self.Ny * self.Nz if n > 0 else 0
+        self._pml_x = (n, n) if slab is None else (slab.pml_lo, slab.pml_hi)
+        self.psi_x_size = sum(self._pml_x) * self.Ny * self.Nz if n > 0 else 0
         self.psi_y_size = self.Nx * 2 * n * self.Nz if n > 0 else 0
         self.psi_z_size = self.Nx * self.Ny * 2 * n if n > 0 else 0
         self.ctx = ctx
@@ -215,19 +228,23 @@ class CUDAFDTD(SourceMonitorMixin):
     def _build_cpml(self):
         torch = _torch()
         n = self.npml
-        prof = build_cpml_profiles((self.Nx, self.Ny, self.Nz), npml=n, dl=self.dl, dt=self.dt,
+        prof = build_cpml_profiles(self.global_shape, npml=n, dl=self.dl, dt=self.dt,
                                    dtype=self.dtype)
         self.cpml_profiles = prof
         up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)  # noqa: E731
+        xs = slice(self.x0, self.x0 + self.Nx)  # a slab's planes of the x profiles
         self._cp = {}
         for stag, axes in (("h", prof.h), ("e", prof.e)):
-            self._cp[stag] = [(up(p.b), up(p.c), up(inverse_kappa_dl(p.kappa, self.dl,
-                                                                      self.dtype)))
-                              for p in axes]
+            self._cp[stag] = [(up(p.b[xs] if a == 0 else p.b), up(p.c[xs] if a == 0 else p.c),
+                               up(inverse_kappa_dl(p.kappa[xs] if a == 0 else p.kappa, self.dl,
+                                                   self.dtype)))
+                              for a, p in enumerate(axes)]
         nx, ny, nz = self.Nx, self.Ny, self.Nz
-        sx, sy, sz = (2 * n, ny, nz), (nx, 2 * n, nz), (nx, ny, 2 * n)
+        sx, sy, sz = (sum(self._pml_x), ny, nz), (nx, 2 * n, nz), (nx, ny, 2 * n)
         if n == 0:
             sx = sy = sz = (1,)
+        if sx[0] == 0:
+            sx = (1,)  # a slab without x-CPML faces: the stripe is never indexed
         mk = lambda s: torch.zeros(s, dtype=self._tdt, device=self.device)  # noqa: E731
         order = (sy, sz, sx, sz, sx, sy)  # Hx_y, Hx_z, Hy_x, Hy_z, Hz_x, Hz_y / E likewise
         with torch.cuda.stream(self.queue):
@@ -238,6 +255,10 @@ class CUDAFDTD(SourceMonitorMixin):
         g = capi.Grid()
         g.nx, g.ny, g.nz, g.npml = self.Nx, self.Ny, self.Nz, self.npml
         g.dtype = capi.FDTD_F32 if self.dtype == np.float32 else capi.FDTD_F64
+        if self.slab is not None:
+            g.x_slab = 1
+            g.pml_x_lo, g.pml_x_hi = self._pml_x
+            g.ghost_lo, g.ghost_hi = self.slab.ghost_lo, self.slab.ghost_hi
         g.lossy = 1 if self.lossy else 0
         g.dtm = self.dt / MU0
         g.dtm_dl = self.dt / (MU0 * self.dl)
@@ -291,7 +312,7 @@ class CUDAFDTD(SourceMonitorMixin):
         rounded coefficients are identical to ``yee_edge_ce`` / ``yee_edge_ca_cb``.
         """
         torch = _torch()
-        expected = (self.Nx, self.Ny, self.Nz)
+        expected = self.global_shape
         if tuple(np.shape(eps_array)) != expected:
             raise ValueError(
                 f"Epsilon shape mismatch: expected {expected}, got {tuple(np.shape(eps_array))}")
@@ -299,8 +320,9 @@ class CUDAFDTD(SourceMonitorMixin):
             raise ValueError(f"Sigma shape mismatch: expected {expected}, "
                              f"got {tuple(np.shape(sigma_array))}")
         self._materialize()
-        eps = np.asarray(eps_array)
-        sig = None if sigma_array is None else np.asarray(sigma_array)
+        xs = slice(self.x0, self.x0 + self.Nx)  # a slab's planes (ghosts included)
+        eps = np.asarray(eps_array)[xs]
+        sig = None if sigma_array is None else np.asarray(sigma_array)[xs]
         narrow = eps.dtype == np.float32 and (sig is None or sig.dtype == np.float32)
         src = np.float32 if narrow else np.float64
         with torch.cuda.stream(self.queue):
@@ -325,7 +347,12 @@ class CUDAFDTD(SourceMonitorMixin):
 
     # ---------------------------------------------------------------- sources
     def _sheet(self, i0, i1, j0, j1):
-        return (0 if i0 is None else int(i0), self.Nx if i1 is None else int(i1),
+        """Sheet bounds in local indices (a slab shifts global i by its first plane;
+        the kernels apply the sheet to local cells only, rim weights still at the
+        sheet's own edges)."""
+        i0 = 0 if i0 is None else int(i0)
+        i1 = self.global_shape[0] if i1 is None else int(i1)
+        return (i0 - self.x0, i1 - self.x0,
                 0 if j0 is None else int(j0), self.Ny if j1 is None else int(j1))
 
     def add_source_Ex(self, z_src, amp, i0=None, i1=None, j0=None, j1=None):

@@ -230,6 +230,9 @@ class CUDANear2FarMonitor:
 
     def __init__(self, fdtd, center, size, freq):
         torch = _torch()
+        if getattr(fdtd, "slab", None) is not None:
+            raise NotImplementedError("the Huygens-box monitor runs on a whole grid, not on one "
+                                      "x-slab of a decomposed grid")
         self.fdtd = fdtd
         self.freqs = np.atleast_1d(np.asarray(freq, dtype=np.float64))
         if not 0 < self.freqs.size <= capi.FDTD_MAX_FREQS:

@@ -180,3 +180,80 @@ def _copy(dst, src):
         dst.copy_(src)
     else:
         dst[...] = src
+
+
+class SlabFDTD:
+    """This rank's slab of an x-decomposed grid, one rank per GPU.
+
+    ``torch.distributed`` must be initialised (NCCL for GPUs); rank r of the
+    group holds slab r of ``partition(shape[0], world, npml)`` on its current
+    CUDA device.  The API follows ``CUDAFDTD`` for what a slab supports:
+    ``set_epsilon`` (the whole grid's εr; each rank takes its planes),
+    ``add_source`` (callbacks get the slab engine, whose ``add_source_Jx`` /
+    ``add_source_Ex`` take global indices), ``step`` / ``run`` (one local step,
+    then the ghost exchange), and ``gather(name)`` (the whole field on rank 0).
+    Every rank calls every method in the same order.
+    """
+
+    def __init__(self, shape, dl, npml=20, dtype=None, *, courant=None, group=None,
+                 fused=True):
+        import numpy as np
+        import torch
+        import torch.distributed as dist
+
+        from .engine import CUDAFDTD
+
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.slab = partition(int(shape[0]), self.world, int(npml))[self.rank]
+        self.engine = CUDAFDTD(shape, dl, npml=npml, dtype=np.float32 if dtype is None else dtype,
+                               courant=courant, device=torch.cuda.current_device(),
+                               fused=fused, slab=self.slab)
+        self._send, self._recv, self._wait = dist_transport(group)
+
+    def set_epsilon(self, eps, sigma_array=None):
+        self.engine.set_epsilon(eps, sigma_array=sigma_array)
+
+    def add_source(self, cb):
+        return self.engine.add_source(cb)
+
+    def add_monitor(self, cb):
+        return self.engine.add_monitor(cb)
+
+    @property
+    def t(self):
+        return self.engine.t
+
+    @property
+    def dt(self):
+        return self.engine.dt
+
+    def _plane(self, name, i):
+        return self.engine.field_tensor(name)[i]
+
+    def step(self):
+        self.engine.step()
+        exchange_ghosts(self.slab, self._plane, self._send, self._recv)
+        self._wait()
+
+    def run(self, n_steps):
+        for _ in range(int(n_steps)):
+            self.step()
+
+    def gather(self, name):
+        """Field ``name`` of the whole grid as a host array on rank 0 (None on the
+        others): every rank sends its owned planes."""
+        import torch
+        import torch.distributed as dist
+
+        own = self.engine.field_tensor(name)[self.slab.owned].contiguous()
+        sizes = [s.g1 - s.g0 for s in partition(self.slab.nx, self.world, self.slab.npml)]
+        if self.rank == 0:
+            parts = [own] + [torch.empty((n,) + tuple(own.shape[1:]), dtype=own.dtype,
+                                         device=own.device) for n in sizes[1:]]
+            for r in range(1, self.world):
+                dist.recv(parts[r], r, group=self.group)
+            return torch.cat(parts).cpu().numpy()
+        dist.send(own, 0, group=self.group)
+        return None
