@@ -257,9 +257,14 @@ int fdtd_n2f_contract(const fdtd_n2f_face *faces, int32_t nfaces, int32_t cur_dt
  * where B, F are the backward / forward differences of yee_update.cl:145-150
  * and :30-35 (zero at index 0 / at the last index). */
 
-/* Adjoint state.  E/H are updated in place; the P stripes have the ψ stripe
- * shapes and order of fdtd_cpml and are ping-ponged: a step reads pe/ph and
- * writes pe_next/ph_next (which must not alias them). */
+/* Adjoint state.  The P stripes have the ψ stripe shapes and order of
+ * fdtd_cpml and are ping-ponged: a step reads pe/ph and writes pe_next/ph_next
+ * (which must not alias them).  With E_next/H_next NULL, E/H are updated in
+ * place by one-thread-per-cell kernels.  With all six set (not aliasing E/H),
+ * a step reads E/H and writes E_next/H_next: the CPML-free interior runs as one
+ * TMA plane march (Ē, H̄, ce read once, Ē', H̄' written once) concurrently with
+ * the CPML shell; the caller swaps the buffers after each step.  Both forms
+ * give the same values bit for bit. */
 typedef struct {
     void *E[3];
     void *H[3];
@@ -268,6 +273,8 @@ typedef struct {
     const void *ph[6];
     void *ph_next[6];
     const void *ce[3];      /* the forward's dt/(eps0 eps_edge)                */
+    void *E_next[3];        /* NULL (in place) or the step's Ē output          */
+    void *H_next[3];        /* NULL (in place) or the step's H̄ output          */
 } fdtd_adjoint_fields;
 
 /* Adjoint source of a real objective J(D) of plane-DFT samples
@@ -369,7 +376,7 @@ const char *fdtd_last_error(void);
 
 /* Device-side error flags raised by kernels since the last reset (bit 0: a
  * bounded wait in the fused step timed out; bit 1: one in the near-to-far
- * contraction did).  Synchronises with the device to
+ * contraction did; bit 2: one in the adjoint interior march did).  Synchronises with the device to
  * read the flag; clears it when reset != 0.  No reference counterpart (the
  * reference kernels have no device-side waits). */
 int fdtd_device_status(int32_t *flags, int32_t reset);

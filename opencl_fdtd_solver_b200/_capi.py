@@ -75,7 +75,7 @@ class Box(Structure):
 
 class AdjointFields(Structure):
     _fields_ = [("E", V3), ("H", V3), ("pe", V6), ("pe_next", V6), ("ph", V6), ("ph_next", V6),
-                ("ce", V3)]
+                ("ce", V3), ("E_next", V3), ("H_next", V3)]
 
 
 class AdjointSeed(Structure):

@@ -151,12 +151,17 @@ class EpsilonAdjoint:
                        checkpoint and replay; ``"all"`` or ``"replay"`` force a mode
     capture_budget   : bytes the ``"auto"`` mode may hold (default: a quarter of the
                        device memory free at the forward call)
+    fused_reverse    : run each reverse step as the interior plane march beside the
+                       CPML-shell kernels, reading one Ē/H̄ buffer pair and writing the
+                       other (default); False updates Ē/H̄ in place with one thread per
+                       cell.  Both give the same gradient bit for bit.
 
     The engine's own monitors are detached while this object steps it.
     """
 
     def __init__(self, fdtd, design, n_steps, objective, *, eps_background=None,
-                 checkpoint_every=100, capture="auto", capture_budget=None):
+                 checkpoint_every=100, capture="auto", capture_budget=None,
+                 fused_reverse=True):
         if not isinstance(fdtd, CUDAFDTD):
             raise TypeError("EpsilonAdjoint needs a CUDAFDTD engine")
         self.fdtd = fdtd
@@ -174,6 +179,7 @@ class EpsilonAdjoint:
         if capture not in ("auto", "all", "replay"):
             raise ValueError(f"capture must be 'auto', 'all' or 'replay', got {capture!r}")
         self.capture = capture
+        self.fused_reverse = bool(fused_reverse)
         self.capture_budget = None if capture_budget is None else int(capture_budget)
         if not isinstance(objective, DFTObjective):
             raise TypeError("objective must be a DFTObjective")
@@ -287,22 +293,30 @@ class EpsilonAdjoint:
 
     # ---------------------------------------------------------------- backward
     def _adjoint_buffers(self):
+        """Ē, H̄ (two sets when the reverse step is fused: it reads one and writes
+        the other) and the two P stripe sets; ``fields[par]`` is the step that
+        reads parity ``par``."""
         fd = self.fdtd
         tdt = fd._tdt
         shp = (fd.Nx, fd.Ny, fd.Nz)
         z = lambda s: torch.zeros(s, dtype=tdt, device=fd.device)  # noqa: E731
-        Eb = [z(shp) for _ in range(3)]
-        Hb = [z(shp) for _ in range(3)]
+        nsets = 2 if self.fused_reverse else 1
+        Eb = [[z(shp) for _ in range(3)] for _ in range(nsets)]
+        Hb = [[z(shp) for _ in range(3)] for _ in range(nsets)]
         stripes = [tuple(p.shape) for p in fd._psi_e]
         PE = [[z(s) for s in stripes] for _ in range(2)]
         PH = [[z(s) for s in stripes] for _ in range(2)]
         fields = []
         for par in range(2):
             f = capi.AdjointFields()
+            cur = par % nsets
             for c in range(3):
-                f.E[c] = Eb[c].data_ptr()
-                f.H[c] = Hb[c].data_ptr()
+                f.E[c] = Eb[cur][c].data_ptr()
+                f.H[c] = Hb[cur][c].data_ptr()
                 f.ce[c] = fd._ce[c].data_ptr()
+                if nsets == 2:
+                    f.E_next[c] = Eb[cur ^ 1][c].data_ptr()
+                    f.H_next[c] = Hb[cur ^ 1][c].data_ptr()
             for q in range(6):
                 f.pe[q] = PE[par][q].data_ptr()
                 f.pe_next[q] = PE[par ^ 1][q].data_ptr()
@@ -310,6 +324,12 @@ class EpsilonAdjoint:
                 f.ph_next[q] = PH[par ^ 1][q].data_ptr()
             fields.append(f)
         return Eb, Hb, PE, PH, fields
+
+    @staticmethod
+    def _state_at(Eb, Hb, par):
+        """The Ē, H̄ tensors that hold the state read by a step of parity ``par``."""
+        k = par % len(Eb)
+        return Eb[k], Hb[k]
 
     def backward(self, grad_output=1.0):
         """``grad_output · ∂J/∂εr`` over the design box (float64 NumPy array)."""
@@ -336,7 +356,7 @@ class EpsilonAdjoint:
         buf = cap[0].numel() * cap.element_size()
         cap0 = cap.data_ptr()
         grid, cpml = fd._grid, fd._cpml_base
-        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb])
+        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb[0]])
         # the reverse sweep runs on its own stream, concurrently with the replay
         # of the next-older segment on the engine's stream
         adj = torch.cuda.Stream(device=fd.device)
@@ -401,7 +421,7 @@ class EpsilonAdjoint:
             fd._monitors = saved
             adj.synchronize()
             fd.queue.synchronize()
-        self._adjoint_state = (Eb, Hb)
+        self._adjoint_state = self._state_at(Eb, Hb, par)
         g_edges = G.cpu().numpy()
         return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)
 
@@ -438,7 +458,7 @@ class EpsilonAdjoint:
         cap0 = self._cap_all.data_ptr()
         slot = self._cap_all[0].numel() * self._cap_all.element_size()
         grid, cpml = fd._grid, fd._cpml_base
-        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb])
+        Ebp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in Eb[0]])
         sd.phase = ph0 + (N - 1) * ph_stride
         capi.run("fdtd_adjoint_seed_add", grid, Ebp, sd, st)
         par = 0
@@ -453,7 +473,7 @@ class EpsilonAdjoint:
             capi.run("fdtd_adjoint_step", grid, fields[par], cpml, gb, seed_arg, st)
             par ^= 1
         fd.queue.synchronize()
-        self._adjoint_state = (Eb, Hb)
+        self._adjoint_state = self._state_at(Eb, Hb, par)
         g_edges = G.cpu().numpy()
         return float(grad_output) * edge_to_cells(g_edges, self._eps, self.design, self.box)
 

@@ -35,6 +35,7 @@
 #include "launch_count.cuh"
 #include "../../include/fdtd_b200.h"
 #include "adjoint.cuh"
+#include "shell_plan.cuh"
 
 namespace fdtd {
 
@@ -140,14 +141,12 @@ __device__ __forceinline__ void adj_grad_cell(const AdjGrad<T> &gb, int i, int j
     }
 }
 
-// Transposed E update: H̄ += B^T ḡ(Ē, P_E); P_E advanced; gradient accumulated.
+// Transposed E update of cell (i, j, k): H̄ += B^T ḡ(Ē, P_E) into Hout (Hout
+// == a.H updates in place), P_E advanced, gradient accumulated.
 template <typename T>
-__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<T> gb) {
-    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
-    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
-    const int i = blockIdx.z;
+__device__ __forceinline__ void adj_h_cell(const AdjArgs<T> &a, const AdjGrad<T> &gb, int i,
+                                           int j, int k, T *const *Hout) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (k >= nz || j >= ny) return;
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T ex = a.E[0][idx], ey = a.E[1][idx], ez = a.E[2][idx];
@@ -166,9 +165,9 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<
         const T g5n = -(a.ce[2][idx + sy] * iky1 * a.E[2][idx + sy]);
         const T g2n = -(a.ce[1][idx + sx] * ikx1 * a.E[1][idx + sx]);
         const T g4n = a.ce[2][idx + sx] * ikx1 * a.E[2][idx + sx];
-        a.H[0][idx] = a.H[0][idx] + ((g3 - g3n) + (g5 - g5n));
-        a.H[1][idx] = a.H[1][idx] + ((g1 - g1n) + (g4 - g4n));
-        a.H[2][idx] = a.H[2][idx] + ((g0 - g0n) + (g2 - g2n));
+        Hout[0][idx] = a.H[0][idx] + ((g3 - g3n) + (g5 - g5n));
+        Hout[1][idx] = a.H[1][idx] + ((g1 - g1n) + (g4 - g4n));
+        Hout[2][idx] = a.H[2][idx] + ((g0 - g0n) + (g2 - g2n));
         if (gb.active) adj_grad_cell(gb, i, j, k, ex, ey, ez);
         return;
     }
@@ -197,23 +196,21 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_H(AdjArgs<T> a, AdjGrad<
     const T tx4 = (i >= 1 ? g4 : T(0)) - g4n;
     const T ty0 = (j >= 1 ? g0 : T(0)) - g0n;
     const T tx2 = (i >= 1 ? g2 : T(0)) - g2n;
-    a.H[0][idx] = a.H[0][idx] + (tz3 + ty5);
-    a.H[1][idx] = a.H[1][idx] + (tz1 + tx4);
-    a.H[2][idx] = a.H[2][idx] + (ty0 + tx2);
+    Hout[0][idx] = a.H[0][idx] + (tz3 + ty5);
+    Hout[1][idx] = a.H[1][idx] + (tz1 + tx4);
+    Hout[2][idx] = a.H[2][idx] + (ty0 + tx2);
     if (gb.active) adj_grad_cell(gb, i, j, k, ex, ey, ez);
 }
 
-// Transposed H update: Ē += F^T ā(H̄, P_H); P_H advanced; then the next seed.
+// Transposed H update of cell (i, j, k): Ē += F^T ā(H̄, P_H) into Eout, with H̄
+// (already advanced this step) read from Hin; P_H advanced; then the seed.
 template <typename T>
-__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed sd) {
-    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
-    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
-    const int i = blockIdx.z;
+__device__ __forceinline__ void adj_e_cell(const AdjArgs<T> &a, const AdjSeed &sd, int i, int j,
+                                           int k, T *const *Hin, T *const *Eout) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (k >= nz || j >= ny) return;
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
-    const T hx = a.H[0][idx], hy = a.H[1][idx], hz = a.H[2][idx];
+    const T hx = Hin[0][idx], hy = Hin[1][idx], hz = Hin[2][idx];
     const int np = a.npml;
     if (np >= 1 && i > np && i < nx - np && j > np && j < ny - np && k > np && k < nz - np) {
         // the cell and its -1 neighbours lie in no slab: h_pair without P terms
@@ -222,19 +219,19 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed 
         const T dm = a.dtm;
         const T a0 = -(dm * iky * hx), a1 = dm * ikz * hx, a2 = dm * ikx * hy;
         const T a3 = -(dm * ikz * hy), a4 = -(dm * ikx * hz), a5 = dm * iky * hz;
-        const T a1p = dm * ikz1 * a.H[0][idx - 1];
-        const T a3p = -(dm * ikz1 * a.H[1][idx - 1]);
-        const T a0p = -(dm * iky1 * a.H[0][idx - sy]);
-        const T a5p = dm * iky1 * a.H[2][idx - sy];
-        const T a2p = dm * ikx1 * a.H[1][idx - sx];
-        const T a4p = -(dm * ikx1 * a.H[2][idx - sx]);
+        const T a1p = dm * ikz1 * Hin[0][idx - 1];
+        const T a3p = -(dm * ikz1 * Hin[1][idx - 1]);
+        const T a0p = -(dm * iky1 * Hin[0][idx - sy]);
+        const T a5p = dm * iky1 * Hin[2][idx - sy];
+        const T a2p = dm * ikx1 * Hin[1][idx - sx];
+        const T a4p = -(dm * ikx1 * Hin[2][idx - sx]);
         T ex = a.E[0][idx] + ((a3p - a3) + (a5p - a5));
         T ey = a.E[1][idx] + ((a1p - a1) + (a4p - a4));
         T ez = a.E[2][idx] + ((a0p - a0) + (a2p - a2));
         if (sd.active) add_seed<T>(sd, i, j, k, ex, ey, ez);
-        a.E[0][idx] = ex;
-        a.E[1][idx] = ey;
-        a.E[2][idx] = ez;
+        Eout[0][idx] = ex;
+        Eout[1][idx] = ey;
+        Eout[2][idx] = ez;
         return;
     }
     const T a0 = h_pair<T, 0, true>(a, i, j, k, hx);
@@ -245,16 +242,16 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed 
     const T a5 = h_pair<T, 5, true>(a, i, j, k, hz);
     T a1p = T(0), a3p = T(0), a0p = T(0), a5p = T(0), a2p = T(0), a4p = T(0);
     if (k >= 1) {
-        a1p = h_pair<T, 1, false>(a, i, j, k - 1, a.H[0][idx - 1]);
-        a3p = h_pair<T, 3, false>(a, i, j, k - 1, a.H[1][idx - 1]);
+        a1p = h_pair<T, 1, false>(a, i, j, k - 1, Hin[0][idx - 1]);
+        a3p = h_pair<T, 3, false>(a, i, j, k - 1, Hin[1][idx - 1]);
     }
     if (j >= 1) {
-        a0p = h_pair<T, 0, false>(a, i, j - 1, k, a.H[0][idx - sy]);
-        a5p = h_pair<T, 5, false>(a, i, j - 1, k, a.H[2][idx - sy]);
+        a0p = h_pair<T, 0, false>(a, i, j - 1, k, Hin[0][idx - sy]);
+        a5p = h_pair<T, 5, false>(a, i, j - 1, k, Hin[2][idx - sy]);
     }
     if (i >= 1) {
-        a2p = h_pair<T, 2, false>(a, i - 1, j, k, a.H[1][idx - sx]);
-        a4p = h_pair<T, 4, false>(a, i - 1, j, k, a.H[2][idx - sx]);
+        a2p = h_pair<T, 2, false>(a, i - 1, j, k, Hin[1][idx - sx]);
+        a4p = h_pair<T, 4, false>(a, i - 1, j, k, Hin[2][idx - sx]);
     }
     const T fz3 = a3p - (k <= nz - 2 ? a3 : T(0));
     const T fy5 = a5p - (j <= ny - 2 ? a5 : T(0));
@@ -266,9 +263,48 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ) k_adj_E(AdjArgs<T> a, AdjSeed 
     T ey = a.E[1][idx] + (fz1 + fx4);
     T ez = a.E[2][idx] + (fy0 + fx2);
     if (sd.active) add_seed<T>(sd, i, j, k, ex, ey, ez);
-    a.E[0][idx] = ex;
-    a.E[1][idx] = ey;
-    a.E[2][idx] = ez;
+    Eout[0][idx] = ex;
+    Eout[1][idx] = ey;
+    Eout[2][idx] = ez;
+}
+
+// Grid-wide reverse half steps: one thread per cell (k fastest), updating
+// in place (Hout = a.H, Hin = Eout... = a.E) or into separate outputs.
+template <typename T>
+__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ)
+    k_adj_H(AdjArgs<T> a, AdjGrad<T> gb, AdjOut<T> out) {
+    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
+    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
+    if (k >= a.nz || j >= a.ny) return;
+    adj_h_cell<T>(a, gb, blockIdx.z, j, k, out.H);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ADJ_TK *ADJ_TJ)
+    k_adj_E(AdjArgs<T> a, AdjSeed sd, AdjOut<T> out) {
+    const int k = blockIdx.x * ADJ_TK + threadIdx.x;
+    const int j = blockIdx.y * ADJ_TJ + threadIdx.y;
+    if (k >= a.nz || j >= a.ny) return;
+    adj_e_cell<T>(a, sd, blockIdx.z, j, k, out.H, out.E);
+}
+
+// Shell reverse half steps: the cells of box o outside box b (shell_plan.cuh).
+template <typename T>
+__global__ void __launch_bounds__(SHELL_THREADS)
+    k_adj_shell_H(AdjArgs<T> a, AdjGrad<T> gb, AdjOut<T> out, ShellPlan sp) {
+    int i, j, k;
+    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
+    adj_h_cell<T>(a, gb, i, j, k, out.H);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SHELL_THREADS)
+    k_adj_shell_E(AdjArgs<T> a, AdjOut<T> out, ShellPlan sp) {
+    int i, j, k;
+    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
+    AdjSeed none;
+    none.active = 0;
+    adj_e_cell<T>(a, none, i, j, k, out.H, out.E);
 }
 
 // Seed only (before the first reverse step): one thread per patch cell.
@@ -310,13 +346,48 @@ __global__ void k_capture(int ny, int nz, const T *E0, const T *E1, const T *E2,
 template <typename T>
 cudaError_t launch_adjoint_step(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjSeed &sd,
                                 cudaStream_t st) {
+    AdjOut<T> out;
+    for (int c = 0; c < 3; ++c) {
+        out.E[c] = a.E[c];
+        out.H[c] = a.H[c];
+    }
+    return launch_adjoint_grid<T>(a, gb, sd, out, st);
+}
+
+template <typename T>
+cudaError_t launch_adjoint_grid(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjSeed &sd,
+                                const AdjOut<T> &out, cudaStream_t st) {
     dim3 blk(ADJ_TK, ADJ_TJ, 1);
     dim3 grd((a.nz + ADJ_TK - 1) / ADJ_TK, (a.ny + ADJ_TJ - 1) / ADJ_TJ, a.nx);
-    k_adj_H<T><<<grd, blk, 0, st>>>(a, gb);
+    k_adj_H<T><<<grd, blk, 0, st>>>(a, gb, out);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_adj_E<T><<<grd, blk, 0, st>>>(a, sd);
+    k_adj_E<T><<<grd, blk, 0, st>>>(a, sd, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_adjoint_shell_H(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjOut<T> &out,
+                                   const ShellBox &o, const ShellBox &b, cudaStream_t st) {
+    if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
+    const ShellPlan sp = make_plan(o, b);
+    const unsigned nb = shell_blocks(sp);
+    if (nb == 0) return cudaSuccess;
+    k_adj_shell_H<T><<<nb, SHELL_THREADS, 0, st>>>(a, gb, out, sp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_adjoint_shell_E(const AdjArgs<T> &a, const AdjOut<T> &out, const ShellBox &o,
+                                   const ShellBox &b, cudaStream_t st) {
+    if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
+    const ShellPlan sp = make_plan(o, b);
+    const unsigned nb = shell_blocks(sp);
+    if (nb == 0) return cudaSuccess;
+    k_adj_shell_E<T><<<nb, SHELL_THREADS, 0, st>>>(a, out, sp);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -352,6 +423,19 @@ template cudaError_t launch_adjoint_step<float>(const AdjArgs<float> &, const Ad
 template cudaError_t launch_adjoint_step<double>(const AdjArgs<double> &,
                                                  const AdjGrad<double> &, const AdjSeed &,
                                                  cudaStream_t);
+#define FDTD_ADJ_INST(T)                                                                   \
+    template cudaError_t launch_adjoint_grid<T>(const AdjArgs<T> &, const AdjGrad<T> &,      \
+                                                const AdjSeed &, const AdjOut<T> &,          \
+                                                cudaStream_t);                               \
+    template cudaError_t launch_adjoint_shell_H<T>(const AdjArgs<T> &, const AdjGrad<T> &,   \
+                                                   const AdjOut<T> &, const ShellBox &,      \
+                                                   const ShellBox &, cudaStream_t);          \
+    template cudaError_t launch_adjoint_shell_E<T>(const AdjArgs<T> &, const AdjOut<T> &,    \
+                                                   const ShellBox &, const ShellBox &,       \
+                                                   cudaStream_t);
+FDTD_ADJ_INST(float)
+FDTD_ADJ_INST(double)
+#undef FDTD_ADJ_INST
 template cudaError_t launch_adjoint_seed<float>(int, int, int, float *const[3], const AdjSeed &,
                                                 cudaStream_t);
 template cudaError_t launch_adjoint_seed<double>(int, int, int, double *const[3],

@@ -316,6 +316,7 @@ fdtd::AdjArgs<T> make_adj(const fdtd_grid *g, const fdtd_adjoint_fields *f, cons
     a.nz = g->nz;
     a.npml = g->npml;
     a.dtm = (T)g->dtm;
+    a.ik_int = (T)g->inv_dl;
     for (int q = 0; q < 3; ++q) {
         a.E[q] = (T *)f->E[q];
         a.H[q] = (T *)f->H[q];
@@ -334,6 +335,16 @@ fdtd::AdjArgs<T> make_adj(const fdtd_grid *g, const fdtd_adjoint_fields *f, cons
         a.ph_next[q] = (T *)f->ph_next[q];
     }
     return a;
+}
+
+template <typename T>
+fdtd::AdjOut<T> adj_out(const fdtd_adjoint_fields *f) {
+    fdtd::AdjOut<T> o;
+    for (int q = 0; q < 3; ++q) {
+        o.E[q] = (T *)f->E_next[q];
+        o.H[q] = (T *)f->H_next[q];
+    }
+    return o;
 }
 
 template <typename T>
@@ -418,7 +429,8 @@ int fdtd_device_status(int32_t *flags, int32_t reset) {
     if (!flags) return fail(FDTD_ERR_INVALID, "flags is NULL");
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_status(e, "device_status");
-    *flags = fdtd::read_fused_error(reset) | (fdtd::n2f::read_error(reset) ? 2 : 0);
+    *flags = fdtd::read_fused_error(reset) | (fdtd::n2f::read_error(reset) ? 2 : 0) |
+             (fdtd::read_adjoint_error(reset) ? 4 : 0);
     return cuda_status(cudaGetLastError(), "device_status");
 }
 
@@ -652,6 +664,26 @@ int fdtd_adjoint_step(const fdtd_grid *g, const fdtd_adjoint_fields *a, const fd
     fdtd::AdjSeed sd;
     if ((rc = build_seed(g, next_seed, sd))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
+    int nnext = 0;
+    for (int q = 0; q < 3; ++q) nnext += (a->E_next[q] != nullptr) + (a->H_next[q] != nullptr);
+    if (nnext != 0 && nnext != 6)
+        return fail(FDTD_ERR_INVALID, "E_next/H_next must be all set or all NULL");
+    if (nnext == 6) {
+        for (int q = 0; q < 3; ++q)
+            for (int r = 0; r < 3; ++r)
+                if (a->E_next[q] == a->E[r] || a->H_next[q] == a->H[r] ||
+                    a->E_next[q] == a->H[r] || a->H_next[q] == a->E[r])
+                    return fail(FDTD_ERR_INVALID, "E_next/H_next must not alias E/H");
+        if (g->dtype == FDTD_F32)
+            return cuda_status(fdtd::launch_adjoint_step_fused<float>(
+                                   make_adj<float>(g, a, c), make_grad<float>(gb), sd,
+                                   adj_out<float>(a), st),
+                               "adjoint_step");
+        return cuda_status(fdtd::launch_adjoint_step_fused<double>(
+                               make_adj<double>(g, a, c), make_grad<double>(gb), sd,
+                               adj_out<double>(a), st),
+                           "adjoint_step");
+    }
     if (g->dtype == FDTD_F32)
         return cuda_status(fdtd::launch_adjoint_step<float>(make_adj<float>(g, a, c),
                                                             make_grad<float>(gb), sd, st),

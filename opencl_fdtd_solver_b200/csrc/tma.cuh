@@ -1,0 +1,106 @@
+// TMA / mbarrier helpers shared by the plane-marching kernels (the forward
+// interior kernel in yee_fused.cu and the adjoint interior kernel in
+// adjoint_fused.cu), the host-side tensor-map cache and the per-thread side
+// stream on which CPML-shell kernels run beside them.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fdtd {
+
+template <typename T>
+struct VecT;
+template <>
+struct VecT<float> {
+    using type = float4;
+};
+template <>
+struct VecT<double> {
+    using type = double2;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void ld_vec(const T *p, T (&out)[V]) {
+    using VT = typename VecT<T>::type;
+    const VT v = *reinterpret_cast<const VT *>(p);
+    const T *q = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int e = 0; e < V; ++e) out[e] = q[e];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
+    using VT = typename VecT<T>::type;
+    VT v;
+    T *q = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int e = 0; e < V; ++e) q[e] = in[e];
+    *reinterpret_cast<VT *>(p) = v;
+}
+
+
+// 3-D tiled tensor map (x = z-index fastest, y = j, z = i) of an (nx, ny, nz)
+// array of elem-byte values with a box of b0 x b1 x 1, no swizzle, no
+// multicast; cached by (base, shape, elem, box).  False if the driver's encoder
+// is unavailable or rejects the map.
+bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem,
+                     int b0, int b1);
+
+// A stream of this host thread and device, with events to fork from and join
+// back to a caller's stream.  slot 0 serves the forward step, slot 1 the
+// adjoint step, so the two can run on different caller streams concurrently.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+cudaError_t side_stream(SideStream **out, int slot = 0);
+
+}  // namespace fdtd

@@ -59,6 +59,7 @@
 #include <unordered_map>
 
 #include "launch_count.cuh"
+#include "tma.cuh"
 #include "yee_launch.cuh"
 
 namespace fdtd {
@@ -75,17 +76,6 @@ struct alignas(64) FusedMaps {
     CUtensorMap H[3];
     CUtensorMap C[3];
     CUtensorMap A[3];
-};
-
-template <typename T>
-struct VecT;
-template <>
-struct VecT<float> {
-    using type = float4;
-};
-template <>
-struct VecT<double> {
-    using type = double2;
 };
 
 template <typename T>
@@ -110,44 +100,6 @@ struct Tile {
     __host__ __device__ static constexpr uint32_t tx_eonly() { return 3u * EW * EH * sizeof(T); }
 };
 
-// ---------------------------------------------------------------- PTX helpers
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
 // Bounded wait: false (and the device error flag set) if the phase did not
 // complete within `limit` polls (the launch's InteriorBox::wait_polls,
 // WAIT_LIMIT unless a caller lowered it).  A zero limit gives up at once
@@ -161,34 +113,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsign
     }
     atomicOr(&g_fused_error, 1);
     return false;
-}
-
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
-                                            int c0, int c1, int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
-
-template <typename T, int V>
-__device__ __forceinline__ void ld_vec(const T *p, T (&out)[V]) {
-    using VT = typename VecT<T>::type;
-    const VT v = *reinterpret_cast<const VT *>(p);
-    const T *q = reinterpret_cast<const T *>(&v);
-#pragma unroll
-    for (int e = 0; e < V; ++e) out[e] = q[e];
-}
-
-template <typename T, int V>
-__device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
-    using VT = typename VecT<T>::type;
-    VT v;
-    T *q = reinterpret_cast<T *>(&v);
-#pragma unroll
-    for (int e = 0; e < V; ++e) q[e] = in[e];
-    *reinterpret_cast<VT *>(p) = v;
 }
 
 struct InteriorBox {
@@ -525,8 +449,10 @@ struct MapKeyHash {
 std::mutex g_map_mu;
 std::unordered_map<MapKey, CUtensorMap, MapKeyHash> g_maps;
 
-bool make_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem, int b0,
-              int b1) {
+}  // namespace
+
+bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem,
+                     int b0, int b1) {
     MapKey key;
     memset(&key, 0, sizeof(key));
     key.base = base;
@@ -557,6 +483,8 @@ bool make_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int el
     g_maps.emplace(key, *out);
     return true;
 }
+
+namespace {
 
 std::atomic<long long> g_wait_polls{(long long)WAIT_LIMIT};
 
@@ -595,11 +523,11 @@ bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
     const int elem = (int)sizeof(T);
     memset(&maps, 0, sizeof(maps));
     for (int c = 0; c < 3; ++c) {
-        if (!make_map(&maps.E[c], a.E[c], a.nx, a.ny, a.nz, elem, L::EW, L::EH) ||
-            !make_map(&maps.H[c], a.H[c], a.nx, a.ny, a.nz, elem, L::HW, L::HH) ||
-            !make_map(&maps.C[c], a.ce[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
+        if (!make_tensor_map(&maps.E[c], a.E[c], a.nx, a.ny, a.nz, elem, L::EW, L::EH) ||
+            !make_tensor_map(&maps.H[c], a.H[c], a.nx, a.ny, a.nz, elem, L::HW, L::HH) ||
+            !make_tensor_map(&maps.C[c], a.ce[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
             return false;
-        if (a.lossy && !make_map(&maps.A[c], a.ca[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
+        if (a.lossy && !make_tensor_map(&maps.A[c], a.ca[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
             return false;
     }
     return true;
@@ -704,35 +632,35 @@ void prof_end(const std::array<cudaEvent_t, NEV> &ev) {
     g_prof.pending.push_back(ev);
     if (g_prof.pending.size() >= 2048) prof_flush_locked();
 }
-// Side stream (per host thread and device) on which the CPML-shell H kernel
-// and the outer shell-E kernel run concurrently with the interior kernel: they
-// are independent of it (the interior kernel recomputes every H it needs from E
-// and H, and the outer E cells read no H of the interior box), so the
-// latency-bound shell fills the bandwidth the interior kernel leaves.  Joined
-// back to the caller's stream by an event before the rim E cells.
-struct SideStream {
-    cudaStream_t s = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
-};
-thread_local std::unordered_map<int, SideStream> t_side;
+}  // namespace
 
-cudaError_t side_stream(SideStream **out) {
+// Side stream (per host thread, device and slot) on which the CPML-shell H
+// kernel and the outer shell-E kernel run concurrently with the interior
+// kernel: they are independent of it (the interior kernel recomputes every H it
+// needs from E and H, and the outer E cells read no H of the interior box), so
+// the latency-bound shell fills the bandwidth the interior kernel leaves.
+// Joined back to the caller's stream by an event before the rim E cells.
+namespace {
+thread_local std::unordered_map<int, SideStream> t_side;
+}
+
+cudaError_t side_stream(SideStream **out, int slot) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    auto it = t_side.find(dev);
+    const int key = dev * 4 + (slot & 3);
+    auto it = t_side.find(key);
     if (it == t_side.end()) {
         SideStream ss;
         if ((e = cudaStreamCreateWithFlags(&ss.s, cudaStreamNonBlocking)) != cudaSuccess) return e;
         if ((e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming)) != cudaSuccess)
             return e;
-        it = t_side.emplace(dev, ss).first;
+        it = t_side.emplace(key, ss).first;
     }
     *out = &it->second;
     return cudaSuccess;
 }
-}  // namespace
 
 void profile_enable(bool on) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
@@ -842,6 +770,9 @@ template cudaError_t launch_step_fused<float>(const YeeArgs<float> &, const Sour
                                               const PlaneList &, cudaStream_t);
 template cudaError_t launch_step_fused<double>(const YeeArgs<double> &, const SourceList &,
                                                const PlaneList &, cudaStream_t);
+
+unsigned interior_wait_polls() { return (unsigned)g_wait_polls.load(); }
+int interior_chunks(int tiles, int nplanes, int sms) { return choose_chunks(tiles, nplanes, sms); }
 
 void set_interior_wait_polls(int64_t polls) {
     g_wait_polls.store(polls < 0 ? (long long)WAIT_LIMIT

@@ -26,109 +26,11 @@
 #include <cuda_runtime.h>
 
 #include "launch_count.cuh"
+#include "shell_plan.cuh"
 #include "yee_launch.cuh"
 
 namespace fdtd {
 
-// Unsigned 32-bit division by a divisor fixed at launch: a multiply-high and a
-// shift in place of the runtime division sequence (Granlund & Montgomery,
-// "Division by invariant integers using multiplication", PLDI 1994, round-up
-// variant): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
-// n / d = (umulhi(m, n) + n) >> l for every 32-bit n, the sum taken in 64 bits.
-struct FastDiv {
-    unsigned d, m, l;
-};
-
-inline FastDiv make_fastdiv(unsigned d) {
-    FastDiv f;
-    f.d = d ? d : 1u;  // empty groups never divide
-    f.l = 0;
-    while ((1ull << f.l) < f.d) ++f.l;
-    f.m = (unsigned)(((1ull << 32) * ((1ull << f.l) - f.d)) / f.d + 1ull);
-    return f;
-}
-
-__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) {
-    return (unsigned)(((unsigned long long)__umulhi(n, f.m) + n) >> f.l);
-}
-
-// Host-precomputed sizes of the three groups and their divisors.  The cells
-// enumerated are those of the outer box o = [o.lo, o.hi) that lie outside the
-// inner box b = [b.lo, b.hi) (b inside o; lo == hi on every axis means an empty
-// inner box, so the whole outer box is enumerated).
-struct ShellPlan {
-    ShellBox b, o;
-    int nax, nay, bx, by, cpr, oy, oz;  // slab planes in x, slab rows in y, inner extents,
-                                        // C cells per row, outer extents in y and z
-    unsigned nA, nB, nC;                // cells per group
-    FastDiv d_plane, d_nz, d_slab, d_cpr, d_by;  // oy*oz, oz, nay*oz, cpr, by
-};
-
-__device__ __forceinline__ bool shell_cell(unsigned t, const ShellPlan &s, int &i, int &j,
-                                           int &k) {
-    const unsigned oz = (unsigned)s.oz;
-    if (t < s.nA) {
-        const unsigned q = fdiv(t, s.d_plane);
-        const unsigned rem = t - q * s.d_plane.d;
-        const int nlo = s.b.lo[0] - s.o.lo[0];
-        i = (int)q < nlo ? s.o.lo[0] + (int)q : s.b.hi[0] + ((int)q - nlo);
-        const unsigned jj = fdiv(rem, s.d_nz);
-        j = s.o.lo[1] + (int)jj;
-        k = s.o.lo[2] + (int)(rem - jj * oz);
-        return true;
-    }
-    t -= s.nA;
-    if (t < s.nB) {
-        const unsigned q = fdiv(t, s.d_slab);
-        const unsigned rem = t - q * s.d_slab.d;
-        i = s.b.lo[0] + (int)q;
-        const unsigned r = fdiv(rem, s.d_nz);
-        const int nlo = s.b.lo[1] - s.o.lo[1];
-        j = (int)r < nlo ? s.o.lo[1] + (int)r : s.b.hi[1] + ((int)r - nlo);
-        k = s.o.lo[2] + (int)(rem - r * oz);
-        return true;
-    }
-    t -= s.nB;
-    if (t < s.nC) {
-        const unsigned row = fdiv(t, s.d_cpr);
-        const int c = (int)(t - row * (unsigned)s.cpr);
-        const unsigned bi = fdiv(row, s.d_by);
-        i = s.b.lo[0] + (int)bi;
-        j = s.b.lo[1] + (int)(row - bi * (unsigned)s.by);
-        const int nlo = s.b.lo[2] - s.o.lo[2];
-        k = c < nlo ? s.o.lo[2] + c : s.b.hi[2] + (c - nlo);
-        return true;
-    }
-    return false;
-}
-
-// An empty inner box (lo == hi == 0 on every axis) enumerates all of o.
-ShellPlan make_plan(const ShellBox &o, const ShellBox &b) {
-    ShellPlan s;
-    s.o = o;
-    s.b = b;
-    if (b.lo[0] == b.hi[0] && b.lo[1] == b.hi[1] && b.lo[2] == b.hi[2])
-        for (int d = 0; d < 3; ++d) s.b.lo[d] = s.b.hi[d] = o.lo[d];
-    const ShellBox &B = s.b;
-    s.oy = o.hi[1] - o.lo[1];
-    s.oz = o.hi[2] - o.lo[2];
-    s.nax = (B.lo[0] - o.lo[0]) + (o.hi[0] - B.hi[0]);
-    s.nay = (B.lo[1] - o.lo[1]) + (o.hi[1] - B.hi[1]);
-    s.bx = B.hi[0] - B.lo[0];
-    s.by = B.hi[1] - B.lo[1];
-    s.cpr = (B.lo[2] - o.lo[2]) + (o.hi[2] - B.hi[2]);
-    s.nA = (unsigned)((int64_t)s.nax * s.oy * s.oz);
-    s.nB = (unsigned)((int64_t)s.bx * s.nay * s.oz);
-    s.nC = (unsigned)((int64_t)s.bx * s.by * s.cpr);
-    s.d_plane = make_fastdiv((unsigned)s.oy * (unsigned)s.oz);
-    s.d_nz = make_fastdiv((unsigned)s.oz);
-    s.d_slab = make_fastdiv((unsigned)s.nay * (unsigned)s.oz);
-    s.d_cpr = make_fastdiv((unsigned)(s.cpr > 0 ? s.cpr : 0));
-    s.d_by = make_fastdiv((unsigned)(s.by > 0 ? s.by : 0));
-    return s;
-}
-
-constexpr int SHELL_THREADS = 256;
 
 template <typename T>
 __global__ void __launch_bounds__(SHELL_THREADS)
@@ -251,26 +153,6 @@ template cudaError_t launch_plane_dft_box<float>(const YeeArgs<float> &, const S
                                                  const PlaneList &, cudaStream_t);
 template cudaError_t launch_plane_dft_box<double>(const YeeArgs<double> &, const ShellBox &,
                                                   const PlaneList &, cudaStream_t);
-
-static unsigned shell_blocks(const ShellPlan &s) {
-    const uint64_t n = (uint64_t)s.nA + s.nB + s.nC;
-    return (unsigned)((n + SHELL_THREADS - 1) / SHELL_THREADS);
-}
-
-static bool plan_fits(const ShellBox &o) {
-    // every group count and the flat index must fit in 32 bits
-    const int64_t ex[3] = {o.hi[0] - o.lo[0], o.hi[1] - o.lo[1], o.hi[2] - o.lo[2]};
-    return ex[0] * ex[1] * ex[2] + SHELL_THREADS < 0xffffffffLL;
-}
-
-static ShellBox whole_grid(int nx, int ny, int nz) {
-    ShellBox o;
-    o.lo[0] = o.lo[1] = o.lo[2] = 0;
-    o.hi[0] = nx;
-    o.hi[1] = ny;
-    o.hi[2] = nz;
-    return o;
-}
 
 template <typename T>
 cudaError_t launch_shell_H(const YeeArgs<T> &a, const ShellBox &b, cudaStream_t st) {
