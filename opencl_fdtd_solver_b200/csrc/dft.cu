@@ -88,20 +88,22 @@ __global__ void k_dft_faces(int nx, int ny, int nz, const T *Ex, const T *Ey, co
         v[3] = quarter * (at(Hx, i, j, k) + at(Hx, i, j, klo) + at(Hx, i, j1, k) + at(Hx, i, j1, klo));
         v[4] = quarter * (at(Hy, i, j, k) + at(Hy, i, j, klo) + at(Hy, i1, j, k) + at(Hy, i1, j, klo));
     }
+    // one frequency per thread (blockIdx.y): the gathers above repeat per
+    // frequency from L1/L2, and the accumulator updates of a warp are coalesced
     const int tang_mask = (c.face <= 1) ? 0x36 : (c.face <= 3) ? 0x2D : 0x1B;
     double2 *A = reinterpret_cast<double2 *>(acc);
+    const int f = blockIdx.y;
+#pragma unroll
     for (int comp = 0; comp < 6; ++comp) {
         if (!(tang_mask & (1 << comp))) continue;
         const double val = (double)v[comp];
         const int h = comp >= 3 ? 2 : 0;
-        for (int f = 0; f < b.nfreq; ++f) {
-            const double pr = phase[4 * f + h], pi = phase[4 * f + h + 1];
-            double2 *a = A + ((int64_t)comp * b.nfreq + f) * b.n_face + s;
-            double2 cur = *a;
-            cur.x = cur.x + val * pr;
-            cur.y = cur.y + val * pi;
-            *a = cur;
-        }
+        const double pr = phase[4 * f + h], pi = phase[4 * f + h + 1];
+        double2 *a = A + ((int64_t)comp * b.nfreq + f) * b.n_face + s;
+        double2 cur = *a;
+        cur.x = cur.x + val * pr;
+        cur.y = cur.y + val * pi;
+        *a = cur;
     }
 }
 
@@ -297,8 +299,9 @@ cudaError_t launch_dft_faces(int nx, int ny, int nz, const T *const E[3], const 
                              const fdtd_box &b, double *acc, const double *phase,
                              cudaStream_t st) {
     const int thr = 128;
-    k_dft_faces<T><<<(b.n_face + thr - 1) / thr, thr, 0, st>>>(nx, ny, nz, E[0], E[1], E[2],
-                                                               H[0], H[1], H[2], b, acc, phase);
+    const dim3 grid((unsigned)((b.n_face + thr - 1) / thr), (unsigned)b.nfreq, 1);
+    k_dft_faces<T><<<grid, thr, 0, st>>>(nx, ny, nz, E[0], E[1], E[2], H[0], H[1], H[2], b, acc,
+                                         phase);
     count_launches(1);
     return cudaGetLastError();
 }

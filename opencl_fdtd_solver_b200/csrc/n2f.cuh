@@ -33,7 +33,7 @@ struct Params {
     uint64_t wait_ns;     // budget of each pipeline wait (0: give up unless already complete)
 };
 
-size_t stage_smem(int mode);
+size_t stage_smem(int mode, bool atm);
 int b_copy_bytes(int mode);
 int k_real_per_step(int mode);
 template <typename CT>

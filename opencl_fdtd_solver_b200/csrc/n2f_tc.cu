@@ -40,6 +40,8 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "launch_count.cuh"
 #include "n2f.cuh"
@@ -52,6 +54,8 @@ __device__ int g_n2f_error;
 constexpr int NGRP = 2;  // phase-generator groups of four warps, on stages g % NGRP
 constexpr int NTHREADS = (6 + 4 * NGRP) * 32;  // B loader, MMA issuer, epilogue, phase groups
 constexpr int MAX_STAGE = 16;
+constexpr int ATM_NST = 6;          // stages when A is in tensor memory (6 x 32 KB of B)
+constexpr uint32_t ATM_ACOL = 256;  // first TMEM column of the A ring (32 per stage)
 constexpr double C0 = 299792458.0;
 
 template <int MODE>
@@ -87,6 +91,8 @@ struct Cfg<FDTD_N2F_TF32> {
     static constexpr uint32_t IDESC =
         (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 };
+static_assert(ATM_NST <= MAX_STAGE && ATM_ACOL + 32 * ATM_NST <= 512 && ATM_ACOL >= BN,
+              "the tensor-memory A ring must fit beside one accumulator in 512 columns");
 static_assert(Cfg<FDTD_N2F_BF16X3>::NST <= MAX_STAGE && Cfg<FDTD_N2F_TF32>::NST <= MAX_STAGE,
               "stage ring larger than the barrier arrays");
 
@@ -174,6 +180,39 @@ __device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t
             "l"(a), "l"(b), "r"(Cfg<MODE>::IDESC), "r"(acc), "r"(z)
             : "memory");
     }
+}
+// The same MMA with A (M x K, one row per TMEM lane, K packed along columns)
+// read from tensor memory instead of shared memory.
+template <int MODE>
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t acc) {
+    if (MODE == FDTD_N2F_BF16X3) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+            "r"(a_tmem), "l"(b), "r"(Cfg<MODE>::IDESC), "r"(acc)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+            "r"(a_tmem), "l"(b), "r"(Cfg<MODE>::IDESC), "r"(acc)
+            : "memory");
+    }
+}
+// Each thread of the warp writes 16 consecutive 32-bit columns of its own lane.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+        "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() {
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -293,13 +332,20 @@ struct Smem {
     int abort_flag;
 };
 
-template <int MODE>
+// ATM: the A operand (phases) lives in tensor memory: the generators write it
+// with tcgen05.st, one row (direction) per TMEM lane, and the MMAs read it from
+// there, so shared memory carries only B (its copies and the MMAs' B reads).
+// TMEM then holds one 128 x 256 accumulator (columns 0-255) and the A ring
+// (columns 256-511, 32 per stage); without ATM the accumulator is
+// double-buffered over the 512 columns and A is in the shared-memory stages.
+template <int MODE, bool ATM>
 __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
     using C = Cfg<MODE>;
-    constexpr int NSTAGE = C::NST;
+    constexpr int NSTAGE = ATM ? ATM_NST : C::NST;
+    constexpr int SSTAGE = ATM ? C::B_COPY : C::STAGE;  // shared-memory bytes per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *stages = smem_raw;
-    Smem *sm = reinterpret_cast<Smem *>(smem_raw + NSTAGE * C::STAGE);
+    Smem *sm = reinterpret_cast<Smem *>(smem_raw + NSTAGE * SSTAGE);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mt = blockIdx.x, fi = blockIdx.y, fr = blockIdx.z;
     const Face &F = P.face[fi];
@@ -342,9 +388,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                     break;
                 const uint32_t bar = smem_u32(&sm->full_b[s]);
                 mbar_arrive_tx(bar, C::B_COPY);
-                bulk_load(smem_u32(stages + s * C::STAGE +
-                                   (MODE == FDTD_N2F_BF16X3 ? 2 : 1) * C::A_BYTES),
-                          src + (int64_t)g * C::B_COPY, C::B_COPY, bar);
+                const int boff = ATM ? 0 : (MODE == FDTD_N2F_BF16X3 ? 2 : 1) * C::A_BYTES;
+                bulk_load(smem_u32(stages + s * SSTAGE + boff), src + (int64_t)g * C::B_COPY,
+                          C::B_COPY, bar);
                 issued = g + 1;
             }
             // every issued copy has landed before the CTA may exit
@@ -358,9 +404,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             int last = -1;  // last stage whose commit was issued
             bool ok = true;
             for (int nt = 0; nt < NT && ok; ++nt) {
-                const int b = nt & 1;
-                if (nt >= 2 &&
-                    !wait_bar(smem_u32(&sm->acc_empty[b]), ((nt >> 1) + 1) & 1, abort_flag, P.wait_ns)) {
+                // ATM: one accumulator, free once the epilogue read tile nt-1;
+                // else two, buffer b free once the epilogue read tile nt-2
+                const int b = ATM ? 0 : (nt & 1);
+                const bool need = ATM ? nt >= 1 : nt >= 2;
+                const uint32_t epar = ATM ? ((nt - 1) & 1) : (((nt >> 1) + 1) & 1);
+                if (need && !wait_bar(smem_u32(&sm->acc_empty[b]), epar, abort_flag, P.wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -375,13 +424,25 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t st = sbase + s * C::STAGE;
+                    const uint32_t st = sbase + s * SSTAGE;
 #pragma unroll
                     for (int m = 0; m < C::MPS; ++m) {
                         // MMA m reads K chunks 2m and 2m+1 of the stage
                         const uint32_t ao = m * 2 * (BM / 8) * 128, bo = m * 2 * (BN / 8) * 128;
                         const uint32_t acc0 = (ks > 0 || m > 0) ? 1u : 0u;
-                        if (MODE == FDTD_N2F_BF16X3) {
+                        if (ATM) {
+                            // A of MMA m: 8 TMEM columns (16 BF16 or 8 TF32 of K) per row
+                            const uint32_t a = tmem + ATM_ACOL + (uint32_t)(s * 32 + m * 8);
+                            if (MODE == FDTD_N2F_BF16X3) {
+                                const uint64_t bhi = make_desc(st + bo, BN * 16, 128);
+                                const uint64_t blo = make_desc(st + C::B_BYTES + bo, BN * 16, 128);
+                                mma_ts<MODE>(d, a, bhi, acc0);
+                                mma_ts<MODE>(d, a, blo, 1u);
+                                mma_ts<MODE>(d, a + 16, bhi, 1u);
+                            } else {
+                                mma_ts<MODE>(d, a, make_desc(st + bo, BN * 16, 128), acc0);
+                            }
+                        } else if (MODE == FDTD_N2F_BF16X3) {
                             const uint64_t ahi = make_desc(st + ao, BM * 16, 128);
                             const uint64_t alo = make_desc(st + C::A_BYTES + ao, BM * 16, 128);
                             const uint64_t bhi = make_desc(st + 2 * C::A_BYTES + bo, BN * 16, 128);
@@ -414,7 +475,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
         // first stage of each n tile and advanced by a float64 rotation of NGRP K
         // steps after that, so each value carries one float rounding.
         const int grp = warp >= 10 ? 1 + (warp - 10) / 4 : 0;
-        const int r = grp ? tid - (320 + 128 * (grp - 1)) : tid - 64;  // 0..127
+        // ATM: the row is the TMEM lane this warp may write (lanes 32*(warp%4) ..)
+        const int r = ATM ? 32 * (warp & 3) + lane
+                          : (grp ? tid - (320 + 128 * (grp - 1)) : tid - 64);  // 0..127
         const int o = mt * BM + r;
         const bool valid = o < P.n_obs;
         const double gp = valid ? freq * F.pitch * P.dirs[3 * o + F.axis_p] / C0 : 0.0;
@@ -430,10 +493,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
             const int s = g % NSTAGE, ks = g % KS;
             if (ks <= prev_ks || prev_ks < 0) U = zphase_turns(gp, (double)(ks * C::PS));
             prev_ks = ks;
-            if (g >= NSTAGE &&
-                !wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag, P.wait_ns))
-                break;
-            unsigned char *st = stages + s * C::STAGE;
+            if (g >= NSTAGE) {
+                bool free_ = wait_bar(smem_u32(&sm->empty[s]), ((g / NSTAGE) - 1) & 1, abort_flag,
+                                      P.wait_ns);
+                // ATM: the warp's tcgen05.st are warp-collective, so it leaves together
+                if (ATM) free_ = __all_sync(0xffffffffu, free_);
+                if (!free_) break;
+                if (ATM) tc_fence_after();
+            }
+            unsigned char *st = stages + s * SSTAGE;
             const float2 uf = make_float2((float)U.x, (float)U.y);
             U = zmul(U, W2);
             float vals[2 * C::PS];
@@ -443,7 +511,37 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                 vals[2 * i] = valid ? u.x : 0.f;
                 vals[2 * i + 1] = valid ? u.y : 0.f;
             }
-            if (MODE == FDTD_N2F_BF16X3) {
+            if (ATM) {
+                // one TMEM row: column c holds K = 2c, 2c+1 (BF16, hi then lo
+                // 16 columns later) or K = c (TF32), the order of the smem rows
+                const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + ATM_ACOL +
+                                    (uint32_t)(s * 32);
+                if (MODE == FDTD_N2F_BF16X3) {
+                    uint32_t hr[16], lr[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(vals[2 * e], vals[2 * e + 1]);
+                        const float2 hf = __bfloat1622float2(h);
+                        const __nv_bfloat162 l =
+                            __floats2bfloat162_rn(vals[2 * e] - hf.x, vals[2 * e + 1] - hf.y);
+                        hr[e] = *reinterpret_cast<const uint32_t *>(&h);
+                        lr[e] = *reinterpret_cast<const uint32_t *>(&l);
+                    }
+                    tmem_st16(ta, hr);
+                    tmem_st16(ta + 16, lr);
+                } else {
+                    uint32_t t0[16], t1[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        t0[e] = __float_as_uint(tf32_rna(vals[e]));
+                        t1[e] = __float_as_uint(tf32_rna(vals[16 + e]));
+                    }
+                    tmem_st16(ta, t0);
+                    tmem_st16(ta + 16, t1);
+                }
+                tmem_st_wait();
+                tc_fence_before();
+            } else if (MODE == FDTD_N2F_BF16X3) {
 #pragma unroll
                 for (int c = 0; c < C::NCH; ++c) {
                     // packed conversions: two values per cvt.rn.bf16x2.f32
@@ -468,7 +566,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
                     *reinterpret_cast<float4 *>(st + c * (BM / 8) * 128 + roff) = v4;
                 }
             }
-            fence_proxy_async();
+            if (!ATM) fence_proxy_async();
             mbar_arrive(smem_u32(&sm->full_a[s]));
         }
     } else {
@@ -494,8 +592,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_n2f_tc(Params P) {
         float2 S[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
                        make_float2(0.f, 0.f)};
         for (int nt = 0; nt < NT; ++nt) {
-            const int b = nt & 1;
-            if (!wait_bar(smem_u32(&sm->acc_full[b]), (nt >> 1) & 1, abort_flag, P.wait_ns)) break;
+            const int b = ATM ? 0 : (nt & 1);
+            const uint32_t fpar = ATM ? (nt & 1) : ((nt >> 1) & 1);
+            // tcgen05.ld is warp-collective: the warp leaves together on a timeout
+            if (!__all_sync(0xffffffffu,
+                            wait_bar(smem_u32(&sm->acc_full[b]), fpar, abort_flag, P.wait_ns)))
+                break;
             tc_fence_after();
             const uint32_t base = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(b * BN);
 #pragma unroll 1
@@ -661,11 +763,24 @@ __global__ void k_n2f_fp64(Params P, double2 *nl) {
 }
 
 // ------------------------------------------------------------------- launchers
-size_t stage_smem(int mode) {
-    const size_t st = mode == FDTD_N2F_BF16X3
-                          ? (size_t)Cfg<FDTD_N2F_BF16X3>::NST * Cfg<FDTD_N2F_BF16X3>::STAGE
-                          : (size_t)Cfg<FDTD_N2F_TF32>::NST * Cfg<FDTD_N2F_TF32>::STAGE;
+size_t stage_smem(int mode, bool atm) {
+    size_t st;
+    if (atm)
+        st = (size_t)ATM_NST * (mode == FDTD_N2F_BF16X3 ? Cfg<FDTD_N2F_BF16X3>::B_COPY
+                                                        : Cfg<FDTD_N2F_TF32>::B_COPY);
+    else
+        st = mode == FDTD_N2F_BF16X3
+                 ? (size_t)Cfg<FDTD_N2F_BF16X3>::NST * Cfg<FDTD_N2F_BF16X3>::STAGE
+                 : (size_t)Cfg<FDTD_N2F_TF32>::NST * Cfg<FDTD_N2F_TF32>::STAGE;
     return st + sizeof(Smem) + 64;
+}
+
+// Where the A operand lives: tensor memory by default; FDTD_B200_N2F_A=smem
+// (read at each call) selects the shared-memory form, with the same MMAs in
+// the same order.
+bool a_in_tmem() {
+    const char *e = getenv("FDTD_B200_N2F_A");
+    return !(e && strcmp(e, "smem") == 0);
 }
 
 int b_copy_bytes(int mode) {
@@ -697,25 +812,28 @@ std::atomic<long long> g_wait_ns{(long long)WAIT_NS};
 
 void set_wait_ns(int64_t ns) { g_wait_ns.store(ns < 0 ? (long long)WAIT_NS : ns); }
 
+template <int MODE, bool ATM>
+static cudaError_t launch_tc(const Params &P, int nfreq, cudaStream_t st) {
+    const size_t smem = stage_smem(MODE, ATM);
+    dim3 grid((P.n_obs + BM - 1) / BM, P.nfaces, nfreq);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_n2f_tc<MODE, ATM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    k_n2f_tc<MODE, ATM><<<grid, NTHREADS, smem, st>>>(P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_contract(int mode, const Params &Pin, int nfreq, cudaStream_t st) {
     Params P = Pin;
     P.wait_ns = (uint64_t)g_wait_ns.load();
-    const size_t smem = stage_smem(mode);
-    dim3 grid((P.n_obs + BM - 1) / BM, P.nfaces, nfreq);
-    cudaError_t e;
-    if (mode == FDTD_N2F_BF16X3) {
-        e = cudaFuncSetAttribute(k_n2f_tc<FDTD_N2F_BF16X3>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_n2f_tc<FDTD_N2F_BF16X3><<<grid, NTHREADS, smem, st>>>(P);
-    } else {
-        e = cudaFuncSetAttribute(k_n2f_tc<FDTD_N2F_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        k_n2f_tc<FDTD_N2F_TF32><<<grid, NTHREADS, smem, st>>>(P);
-    }
-    count_launches(1);
-    return cudaGetLastError();
+    const bool atm = a_in_tmem();
+    if (mode == FDTD_N2F_BF16X3)
+        return atm ? launch_tc<FDTD_N2F_BF16X3, true>(P, nfreq, st)
+                   : launch_tc<FDTD_N2F_BF16X3, false>(P, nfreq, st);
+    return atm ? launch_tc<FDTD_N2F_TF32, true>(P, nfreq, st)
+               : launch_tc<FDTD_N2F_TF32, false>(P, nfreq, st);
 }
 
 cudaError_t launch_combine(const Params &P, int nfreq, float2 *nl, cudaStream_t st) {

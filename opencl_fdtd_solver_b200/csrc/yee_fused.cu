@@ -652,7 +652,15 @@ cudaError_t side_stream(SideStream **out, int slot) {
     auto it = t_side.find(key);
     if (it == t_side.end()) {
         SideStream ss;
-        if ((e = cudaStreamCreateWithFlags(&ss.s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        // FDTD_B200_SIDE_PRIO=1 gives the side stream the device's highest
+        // priority (its blocks are dispatched before the interior kernel's)
+        int lo = 0, hi = 0;
+        const char *pv = getenv("FDTD_B200_SIDE_PRIO");
+        const bool prio = pv && atoi(pv) == 1 && cudaDeviceGetStreamPriorityRange(&lo, &hi) ==
+                                                      cudaSuccess;
+        if ((e = cudaStreamCreateWithPriority(&ss.s, cudaStreamNonBlocking, prio ? hi : 0)) !=
+            cudaSuccess)
+            return e;
         if ((e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming)) != cudaSuccess)
             return e;
@@ -678,6 +686,16 @@ cudaError_t profile_read(double ms[5], int *steps) {
     for (int s = 0; s < NPROF; ++s) ms[s] = g_prof.ms[s];
     *steps = g_prof.steps;
     return e;
+}
+
+// FDTD_B200_SHELL_SPLIT=0 runs all shell E cells after the join instead of
+// splitting off the outer part onto the side stream (a schedule knob).
+bool split_shell_e() {
+    static const bool v = [] {
+        const char *e = getenv("FDTD_B200_SHELL_SPLIT");
+        return !(e && atoi(e) == 0);
+    }();
+    return v;
 }
 
 template <typename T>
@@ -737,7 +755,8 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
             (e = cudaStreamWaitEvent(side->s, side->fork, 0)) == cudaSuccess)
             e = launch_shell_H<T>(a, hbox, side->s);
         if (prof) cudaEventRecord(ev[1], side->s);
-        if (e == cudaSuccess) e = launch_shell_E_region<T>(a, all, rbox, src, pl, side->s);
+        if (e == cudaSuccess && split_shell_e())
+            e = launch_shell_E_region<T>(a, all, rbox, src, pl, side->s);
         if (prof) cudaEventRecord(ev[2], side->s);
         cudaError_t e2 = cudaEventRecord(side->join, side->s);
         if (e == cudaSuccess) e = e2;
@@ -757,8 +776,11 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
     // plane DFTs of the cells the interior kernel updated
     if (e == cudaSuccess && use_interior && pl.n) e = launch_plane_dft_box<T>(a, ebox, pl, st);
     if (prof) cudaEventRecord(ev[5], st);
-    // E of the rim (or of the whole grid without an interior box)
-    if (e == cudaSuccess) e = launch_shell_E_region<T>(a, rbox, ebox, src, pl, st);
+    // E of the rim (or of the whole grid without an interior box), or of every
+    // cell outside B' when the outer part did not run on the side stream
+    if (e == cudaSuccess)
+        e = launch_shell_E_region<T>(a, (use_interior && split_shell_e()) ? rbox : all, ebox, src,
+                                     pl, st);
     if (prof) {
         cudaEventRecord(ev[6], st);
         prof_end(ev);

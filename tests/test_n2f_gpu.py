@@ -133,3 +133,20 @@ def test_monitor_faces_reproduce_engine_far_field():
         ref = dft_oracle.nl_integrals(pos, wda, cur, k, dirs * 10.0)
         assert _rel(nl64[fi], ref) <= 1e-10
         assert _rel(nl16[fi].astype(np.complex128), ref) <= 5e-5
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "tf32"])
+def test_a_operand_in_tensor_memory_equals_shared_memory_form(small, mode, monkeypatch):
+    """The A operand (phases) written to tensor memory and read from there by
+    the MMAs gives the shared-memory form's result bit for bit: the same values,
+    the same K order, the same MMAs in the same order."""
+    from opencl_fdtd_solver_b200.n2f import near2far_contract
+
+    faces, dirs, freqs, _ = small
+    dev = _to_dev(faces)
+    out = {}
+    for where in ("smem", "tmem"):
+        monkeypatch.setenv("FDTD_B200_N2F_A", where)
+        out[where] = near2far_contract(dev, freqs, dirs, mode=mode).cpu().numpy()
+    assert np.abs(out["smem"]).max() > 0
+    assert np.array_equal(out["smem"], out["tmem"])
