@@ -600,6 +600,15 @@ def run_adjoint_leg(args):
     t_fwd = min(timed(lambda: plain_forward(adj, eps_d), st)[0] for _ in range(3))
     t_grad, (J32, g32) = min((timed(lambda: adj.value_and_grad(eps_d), st) for _ in range(3)),
                              key=lambda r: r[0])
+    # the two passes of the gradient apart: forward (with the captures) and the
+    # reverse sweep alone, whose per-step time is the reverse step's
+    t_fwd_cap = timed(lambda: adj.forward(eps_d), st)[0]
+    t_bwd = timed(lambda: adj.backward(), st)[0]
+    # the same reverse sweep with the per-cell in-place kernels (the gradient is
+    # bit-identical; the comparison shows the interior march's effect)
+    adj.fused_reverse = False
+    t_bwd_cell = timed(lambda: adj.backward(), st)[0]
+    adj.fused_reverse = True
     del adj
     torch.cuda.empty_cache()
     adj64 = adjoint_problem(np.float64, args.adj_steps)
@@ -629,6 +638,11 @@ def run_adjoint_leg(args):
         "t_forward_ms": round(t_fwd, 2),
         "t_grad_ms": round(t_grad, 2),
         "grad_cost_forward_solves": round(t_grad / t_fwd, 3),
+        "t_forward_with_captures_ms": round(t_fwd_cap, 2),
+        "t_reverse_sweep_ms": round(t_bwd, 2),
+        "reverse_step_us": round(1e3 * t_bwd / args.adj_steps, 2),
+        "forward_step_us": round(1e3 * t_fwd / args.adj_steps, 2),
+        "reverse_step_us_per_cell_kernels": round(1e3 * t_bwd_cell / args.adj_steps, 2),
         "target_forward_solves": 4,
         "fd_gradient_cost_forward_solves": n_design + 1,
         "fd_gradient_ms_extrapolated": round((n_design + 1) * t_fwd, 1),

@@ -17,11 +17,13 @@
 //
 // Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'):
 //   side stream (slot 1):  k_adj_shell_H on the cells outside HB = [npml,
-//                          N-npml-1)^3, then k_adj_shell_E on the cells outside
-//                          R = [npml, N-npml)^3 (their stencils read no H̄' of HB)
+//                          N-npml-1)^3
 //   caller's stream:       k_adj_interior: H̄' on HB, Ē' on EB = [npml+1, N-npml-1)^3
-//   after the join:        k_adj_shell_E on the rim R \ EB, then the objective's
-//                          seed on Ē' (k_adj_seed), in the order adj_e_cell adds it.
+//   after the join:        k_adj_shell_E on the cells outside EB, then the
+//                          objective's seed on Ē' (k_adj_seed), in the order
+//                          adj_e_cell adds it.  (With the forward step's split
+//                          knob, the Ē cells outside R = [npml, N-npml)^3 run on
+//                          the side stream instead.)
 //
 // Interior kernel: each CTA owns a (TJ x TK) tile of (j, k) and marches along i
 // over a chunk of planes.  Plane p arrives by TMA (cp.async.bulk.tensor 3-D
@@ -51,6 +53,7 @@ namespace fdtd {
 
 unsigned interior_wait_polls();
 int interior_chunks(int tiles, int nplanes, int sms);
+bool split_shell_e();
 
 namespace {
 
@@ -61,10 +64,12 @@ constexpr int A_NCELL = 128;              // 16 vector groups x 8 rows
 constexpr int A_NTHREADS = A_NCELL + 32;  // + one halo warp
 constexpr unsigned A_DRAIN = (1u << 24) / 16;
 
-template <typename T>
+// G vector groups of V cells per row: 16 (TK x TJ = 64 x 8 FP32) or 8 (32 x
+// 16), whichever pads the box's k extent less (same halo ratio and bytes).
+template <typename T, int GG>
 struct ATile {
     static constexpr int V = 16 / (int)sizeof(T);
-    static constexpr int G = 16;
+    static constexpr int G = GG;
     static constexpr int TK = G * V;
     static constexpr int TJ = A_NCELL / G;
     static constexpr int EW = TK + 2 * V, EH = TJ + 2;
@@ -129,11 +134,11 @@ __device__ __forceinline__ void march_grad(const AdjGrad<T> &gb, int i, int j, i
     }
 }
 
-template <typename T, int NSTAGE>
+template <typename T, int NSTAGE, int GG>
 __global__ void __launch_bounds__(A_NTHREADS, 2)
     k_adj_interior(const __grid_constant__ AdjMaps maps, const __grid_constant__ AdjMarch<T> m,
                    const __grid_constant__ AdjBox bx) {
-    using L = ATile<T>;
+    using L = ATile<T, GG>;
     constexpr int V = L::V, TK = L::TK, TJ = L::TJ, EW = L::EW, HW = L::HW;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>(
@@ -390,9 +395,9 @@ __global__ void __launch_bounds__(A_NTHREADS, 2)
     }
 }
 
-template <typename T>
+template <typename T, int GG>
 bool adj_maps(const AdjArgs<T> &a, AdjMaps &maps) {
-    using L = ATile<T>;
+    using L = ATile<T, GG>;
     const int elem = (int)sizeof(T);
     memset(&maps, 0, sizeof(maps));
     for (int c = 0; c < 3; ++c)
@@ -403,10 +408,10 @@ bool adj_maps(const AdjArgs<T> &a, AdjMaps &maps) {
     return true;
 }
 
-template <typename T>
+template <typename T, int GG>
 cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjOut<T> &out,
                                 const AdjMaps &maps, const ShellBox &hb, cudaStream_t st) {
-    using L = ATile<T>;
+    using L = ATile<T, GG>;
     AdjBox bx;
     for (int d = 0; d < 3; ++d) {
         bx.lo[d] = hb.lo[d];
@@ -439,10 +444,10 @@ cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjGrad<T> &gb, const
     }
     m.gb = gb;
     dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
-    cudaError_t e = cudaFuncSetAttribute(k_adj_interior<T, A_NSTAGE>,
+    cudaError_t e = cudaFuncSetAttribute(k_adj_interior<T, A_NSTAGE, GG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_adj_interior<T, A_NSTAGE><<<grid, A_NTHREADS, smem, st>>>(maps, m, bx);
+    k_adj_interior<T, A_NSTAGE, GG><<<grid, A_NTHREADS, smem, st>>>(maps, m, bx);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -463,8 +468,14 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
         for (const void *q : ptrs)
             if (reinterpret_cast<uintptr_t>(q) % 16 != 0) march = false;
     }
+    int gsel = 16;
+    {
+        const int V = ATile<T, 16>::V, k0 = (a.npml / V) * V, ext = (n[2] - a.npml - 1) - k0;
+        const int w16 = ATile<T, 16>::TK, w8 = ATile<T, 8>::TK;
+        if ((ext + w8 - 1) / w8 * w8 < (ext + w16 - 1) / w16 * w16) gsel = 8;
+    }
     AdjMaps maps;
-    if (march && !adj_maps<T>(a, maps)) march = false;
+    if (march && !(gsel == 8 ? adj_maps<T, 8>(a, maps) : adj_maps<T, 16>(a, maps))) march = false;
     if (!march) {
         // grid-wide per-cell kernels into the outputs, then the seed (the same
         // result as the in-place path)
@@ -491,14 +502,17 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
     if (e != cudaSuccess) return e;
     if ((e = cudaEventRecord(side->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(side->s, side->fork, 0)) != cudaSuccess) return e;
+    const bool split = split_shell_e();
     e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, side->s);
-    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, all, rb, side->s);
+    if (e == cudaSuccess && split) e = launch_adjoint_shell_E<T>(a, out, all, rb, side->s);
     cudaError_t e2 = cudaEventRecord(side->join, side->s);
     if (e == cudaSuccess) e = e2;
-    if (e == cudaSuccess) e = launch_adj_interior<T>(a, gb, out, maps, hb, st);
+    if (e == cudaSuccess)
+        e = gsel == 8 ? launch_adj_interior<T, 8>(a, gb, out, maps, hb, st)
+                      : launch_adj_interior<T, 16>(a, gb, out, maps, hb, st);
     e2 = cudaStreamWaitEvent(st, side->join, 0);
     if (e == cudaSuccess) e = e2;
-    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, rb, eb, st);
+    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, split ? rb : all, eb, st);
     if (e == cudaSuccess && sd.active)
         e = launch_adjoint_seed<T>(a.nx, a.ny, a.nz, out.E, sd, st);
     return e;

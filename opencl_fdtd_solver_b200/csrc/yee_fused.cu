@@ -78,12 +78,15 @@ struct alignas(64) FusedMaps {
     CUtensorMap A[3];
 };
 
-template <typename T>
+// Tile of TJ rows (j) x TK cells (k): G vector groups of V cells per row.
+// G = 16: 64 x 8 (FP32) / 32 x 8 (FP64); G = 8: 32 x 16 / 16 x 16, the same
+// halo ratio and shared memory, chosen when it pads the k extent less.
+template <typename T, int GG = 16>
 struct Tile {
     static constexpr int V = 16 / (int)sizeof(T);  // elements per 16-byte vector
-    static constexpr int G = 16;                    // vector groups per row
-    static constexpr int TK = G * V;                // 64 (FP32) or 32 (FP64)
-    static constexpr int TJ = NCELLTHR / G;         // 8
+    static constexpr int G = GG;                    // vector groups per row
+    static constexpr int TK = G * V;
+    static constexpr int TJ = NCELLTHR / G;
     static constexpr int EW = TK + 2 * V, EH = TJ + 2;
     static constexpr int HW = TK + V, HH = TJ + 1;
     __host__ __device__ static constexpr int pad128(int b) { return (b + 127) / 128 * 128; }
@@ -124,11 +127,11 @@ struct InteriorBox {
 };
 
 // ---------------------------------------------------------------- the kernel
-template <typename T, bool LOSSY, int NSTAGE>
+template <typename T, bool LOSSY, int NSTAGE, int GG>
 __global__ void __launch_bounds__(NTHREADS, 2)
     k_interior(const __grid_constant__ FusedMaps maps, const YeeArgs<T> a,
                const __grid_constant__ InteriorBox bx, const __grid_constant__ SourceList src) {
-    using L = Tile<T>;
+    using L = Tile<T, GG>;
     constexpr int V = L::V, TK = L::TK, TJ = L::TJ, EW = L::EW, HW = L::HW;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = reinterpret_cast<unsigned char *>(
@@ -517,9 +520,9 @@ int choose_chunks(int tiles, int nplanes, int sms) {
     return best;
 }
 
-template <typename T>
+template <typename T, int GG>
 bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
-    using L = Tile<T>;
+    using L = Tile<T, GG>;
     const int elem = (int)sizeof(T);
     memset(&maps, 0, sizeof(maps));
     for (int c = 0; c < 3; ++c) {
@@ -533,10 +536,10 @@ bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
     return true;
 }
 
-template <typename T>
+template <typename T, int GG>
 cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const ShellBox &hb,
                             const SourceList &src, cudaStream_t st) {
-    using L = Tile<T>;
+    using L = Tile<T, GG>;
     InteriorBox bx;
     for (int d = 0; d < 3; ++d) {
         bx.lo[d] = hb.lo[d];
@@ -563,10 +566,10 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
     cudaError_t e = cudaSuccess;
 #define FDTD_LAUNCH_INTERIOR(LS, NS)                                                           \
     do {                                                                                       \
-        e = cudaFuncSetAttribute(k_interior<T, LS, NS>,                                        \
+        e = cudaFuncSetAttribute(k_interior<T, LS, NS, GG>,                                    \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
         if (e != cudaSuccess) return e;                                                        \
-        k_interior<T, LS, NS><<<grid, NTHREADS, smem, st>>>(maps, a, bx, src);                 \
+        k_interior<T, LS, NS, GG><<<grid, NTHREADS, smem, st>>>(maps, a, bx, src);             \
         count_launches(1);                                                                     \
     } while (0)
     if (a.lossy) {
@@ -688,12 +691,14 @@ cudaError_t profile_read(double ms[5], int *steps) {
     return e;
 }
 
-// FDTD_B200_SHELL_SPLIT=0 runs all shell E cells after the join instead of
-// splitting off the outer part onto the side stream (a schedule knob).
+// FDTD_B200_SHELL_SPLIT=1 splits the shell E cells whose stencils read no H of
+// B off onto the side stream, behind k_shell_H (measured slower at 512³: the
+// side stream is starved while the interior kernel holds the SMs, 2.05 against
+// 1.88 ms); by default all shell E cells run after the join.
 bool split_shell_e() {
     static const bool v = [] {
         const char *e = getenv("FDTD_B200_SHELL_SPLIT");
-        return !(e && atoi(e) == 0);
+        return e && atoi(e) == 1;
     }();
     return v;
 }
@@ -723,8 +728,17 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
             if (reinterpret_cast<uintptr_t>(q) % 16 != 0) use_interior = false;
         if (a.lossy && reinterpret_cast<uintptr_t>(a.ca[c]) % 16 != 0) use_interior = false;
     }
+    // tile shape: the one that pads the interior's k extent [lo, hi) least
+    // (k0 starts at lo rounded down to a 16-byte boundary)
+    int gsel = 16;
+    {
+        const int k0 = (blo[2] / Tile<T, 16>::V) * Tile<T, 16>::V, ext = bhi[2] - k0;
+        const int w16 = Tile<T, 16>::TK, w8 = Tile<T, 8>::TK;
+        if ((ext + w8 - 1) / w8 * w8 < (ext + w16 - 1) / w16 * w16) gsel = 8;
+    }
     FusedMaps maps;
-    if (use_interior && !build_maps<T>(a, maps)) use_interior = false;
+    if (use_interior && !(gsel == 8 ? build_maps<T, 8>(a, maps) : build_maps<T, 16>(a, maps)))
+        use_interior = false;
     // hbox = B (H of the interior kernel), ebox = B' (its E), rbox = [lo, hi+1):
     // the E cells outside rbox read no H of B, the rim rbox \ B' does
     ShellBox hbox, ebox, rbox, none, all;
@@ -760,7 +774,9 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
         if (prof) cudaEventRecord(ev[2], side->s);
         cudaError_t e2 = cudaEventRecord(side->join, side->s);
         if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = launch_interior<T>(a, maps, hbox, src, st);
+        if (e == cudaSuccess)
+            e = gsel == 8 ? launch_interior<T, 8>(a, maps, hbox, src, st)
+                          : launch_interior<T, 16>(a, maps, hbox, src, st);
         if (prof) cudaEventRecord(ev[3], st);
         e2 = cudaStreamWaitEvent(st, side->join, 0);
         if (e == cudaSuccess) e = e2;
