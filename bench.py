@@ -342,8 +342,8 @@ def run_steps_timed(g, k):
     nsteps = ctypes.c_int32()
     capi.run("fdtd_profile_read", ms, ctypes.byref(nsteps))
     per_kernel = {name: ms[i] / max(1, nsteps.value)
-                  for i, name in enumerate(("k_shell_H", "k_shell_E_outer", "k_interior",
-                                            "k_plane_dft_box", "k_shell_E_rim"))}
+                  for i, name in enumerate(("k_shell_H", "k_shell_E_side", "k_interior",
+                                            "k_plane_dft_box", "k_shell_E"))}
     phases = {f"ms_per_step_first_{split}": round(start.elapsed_time(mid) / max(1, split), 4)}
     if k > split:
         phases[f"ms_per_step_after_{split}"] = round(mid.elapsed_time(end) / (k - split), 4)

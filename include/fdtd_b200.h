@@ -361,10 +361,11 @@ int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int
  * the sums and records CUDA events around every launch of each following
  * fdtd_step on its stream; enable == 0 stops recording.  fdtd_profile_read
  * waits for the recorded events and returns the summed milliseconds per
- * launch, [0] CPML-shell H and [1] the outer CPML-shell E (both on the side
- * stream, concurrent with [2]), [2] the interior single-pass kernel, [3] the
- * plane DFT of the interior, [4] the rim E cells after the join (with sources
- * and DFTs), and the number of steps recorded.  No reference counterpart. */
+ * launch, [0] CPML-shell H on the side stream (concurrent with [2]), [1] the
+ * shell E cells run on the side stream (none unless FDTD_B200_SHELL_SPLIT=1
+ * selects that schedule), [2] the interior single-pass kernel, [3] the plane
+ * DFT of the interior, [4] the shell E cells after the join (with sources and
+ * DFTs), and the number of steps recorded.  No reference counterpart. */
 int fdtd_profile_steps(int32_t enable);
 int fdtd_profile_read(double ms[5], int32_t *nsteps);
 

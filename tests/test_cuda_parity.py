@@ -511,9 +511,10 @@ def test_launch_counter_and_step_profile(cuda):
     n = ctypes.c_int32()
     capi.run("fdtd_profile_read", ms, ctypes.byref(n))
     assert n.value == 5
-    assert all(v > 0 for v in ms)
-    # shell H, outer shell E, interior, plane DFT of the interior, rim E per step
-    assert capi.lib().fdtd_launch_count() - n0 == 5 * 5
+    assert ms[0] > 0 and ms[2] > 0 and ms[3] > 0 and ms[4] > 0
+    # shell H, interior, plane DFT of the interior, shell E per step (the outer
+    # shell E slot records no launch unless the split schedule is selected)
+    assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
 
 
 @pytest.mark.parametrize("steps", [200, 2000], ids=["200_steps", "full_2000_steps"])
