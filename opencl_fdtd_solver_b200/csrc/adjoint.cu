@@ -67,10 +67,14 @@ __device__ __forceinline__ T e_pair(const AdjArgs<T> &a, int i, int j, int k, T 
     const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
     const T t = ce * a.cpe.ik[D][x] * eb;
     T g = POS ? t : -t;
-    if (in_slab(x, n, a.npml)) {
-        const int64_t s = stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml);
+    // the P read is issued whether or not the cell is in the slab (a harmless
+    // valid address otherwise, its value discarded), so it waits behind no branch
+    const bool in = in_slab(x, n, a.npml);
+    const int64_t s = in ? stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml) : 0;
+    const T pold = *(in ? a.pe[P] + s : a.cpe.b[D]);
+    if (in) {
         const T u = ce * eb;
-        const T pn = a.cpe.b[D][x] * a.pe[P][s] + (POS ? u : -u);
+        const T pn = a.cpe.b[D][x] * pold + (POS ? u : -u);
         if (OWN) a.pe_next[P][s] = pn;
         g = g + a.cpe.c[D][x] * pn;
     }
@@ -86,10 +90,12 @@ __device__ __forceinline__ T h_pair(const AdjArgs<T> &a, int i, int j, int k, T 
     const int n = D == 0 ? a.nx : (D == 1 ? a.ny : a.nz);
     const T t = a.dtm * a.cph.ik[D][x] * hb;
     T g = POS ? t : -t;
-    if (in_slab(x, n, a.npml)) {
-        const int64_t s = stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml);
+    const bool in = in_slab(x, n, a.npml);
+    const int64_t s = in ? stripe_index<D>(i, j, k, a.nx, a.ny, a.nz, a.npml) : 0;
+    const T pold = *(in ? a.ph[P] + s : a.cph.b[D]);
+    if (in) {
         const T u = a.dtm * hb;
-        const T pn = a.cph.b[D][x] * a.ph[P][s] + (POS ? u : -u);
+        const T pn = a.cph.b[D][x] * pold + (POS ? u : -u);
         if (OWN) a.ph_next[P][s] = pn;
         g = g + a.cph.c[D][x] * pn;
     }
