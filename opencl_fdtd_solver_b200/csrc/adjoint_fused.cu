@@ -250,12 +250,22 @@ __global__ void __launch_bounds__(A_NTHREADS, 2)
                 uxn = uval(E0x, C0x, eo + V);
                 uyn = uval(E0y, C0y, eo + V);
             }
+            // the j+1 row (x, z) and the i+1 plane (y, z) as 16-byte vectors
+            T exj[V], ezj[V], cxj[V], czj[V], eyi[V], ezi[V], cyi[V], czi[V];
+            ld_vec<T, V>(E0x + eo + EW, exj);
+            ld_vec<T, V>(C0x + eo + EW, cxj);
+            ld_vec<T, V>(E0z + eo + EW, ezj);
+            ld_vec<T, V>(C0z + eo + EW, czj);
+            ld_vec<T, V>(E1y + eo, eyi);
+            ld_vec<T, V>(C1y + eo, cyi);
+            ld_vec<T, V>(E1z + eo, ezi);
+            ld_vec<T, V>(C1z + eo, czi);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const T uxk = (v < V - 1) ? ux[v + 1] : uxn;
                 const T uyk = (v < V - 1) ? uy[v + 1] : uyn;
-                const T uxj = uval(E0x, C0x, eo + EW + v), uzj = uval(E0z, C0z, eo + EW + v);
-                const T uyi = uval(E1y, C1y, eo + v), uzi = uval(E1z, C1z, eo + v);
+                const T uxj = (cxj[v] * ik) * exj[v], uzj = (czj[v] * ik) * ezj[v];
+                const T uyi = (cyi[v] * ik) * eyi[v], uzi = (czi[v] * ik) * ezi[v];
                 hx[v] = hx[v] + ((uy[v] - uyk) + ((-uz[v]) - (-uzj)));
                 hy[v] = hy[v] + (((-ux[v]) - (-uxk)) + (uz[v] - uzi));
                 hz[v] = hz[v] + ((ux[v] - uxj) + ((-uy[v]) - (-uyi)));

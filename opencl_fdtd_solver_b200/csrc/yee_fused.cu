@@ -501,14 +501,17 @@ int stage_count() {
     return n;
 }
 
-// Chunks along i: whole waves of resident CTAs, chunks of at least 16 planes.
+// Chunks along i: whole waves of resident CTAs, chunks of at least 16 planes
+// (8 when there are fewer tiles than resident CTA slots: a small grid needs
+// the shorter marches to fill the GPU, at one extra plane read per chunk).
 int choose_chunks(int tiles, int nplanes, int sms) {
     const int slots = (stage_count() == 3 ? 3 : 2) * sms;
+    const int min_len = tiles < slots ? 8 : 16;
     int best = 1;
     double best_score = -1.0;
     for (int c = 1; c <= 64; ++c) {
         const int len = (nplanes + c - 1) / c;
-        if (len < 16 && c > 1) break;
+        if (len < min_len && c > 1) break;
         const double waves = (double)tiles * c / slots;
         const double fill = waves / std::ceil(waves);
         const double score = fill * (1.0 - 1.0 / (len + 1.0));
