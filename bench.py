@@ -864,7 +864,10 @@ def run_fp64_error_leg(args):
         DFTs and the far field at 20 and 40 GHz (direct and split-BF16), against
         the FP64 CUDA engine (itself within 1e-12 of FP64 NumPy on the parity tests);
       * roofline (512³ blocky εr): the six fields and the Ex plane DFT after
-        ``--fp64-error-steps`` steps, against the FP64 CUDA engine."""
+        ``--fp64-error-steps`` steps, against the FP64 CUDA engine.
+    H errors are also given over η0 times the E peak: the sources leave a static
+    charge field in E near them, H is a difference of those large E values, and
+    its own peak is small once the pulse has left."""
     import torch
 
     from opencl_fdtd_solver_b200 import CUDAFDTD, CUDAPlaneDFTMonitor
@@ -894,8 +897,13 @@ def run_fp64_error_leg(args):
 
     o.add_monitor(plane)
     o.run(500)
+    from opencl_fdtd_solver_b200 import ETA0
+
+    e_peak = np.abs(o.Ex).max()
     out["small_64^3_500steps_vs_fp64_numpy"] = {
         "Ex": _peak_err(g.Ex, o.Ex), "Hy": _peak_err(g.Hy, o.Hy),
+        "Hy_over_eta0_Ex_peak": float(ETA0 * np.abs(g.Hy.astype(np.float64) - o.Hy).max()
+                                      / e_peak),
         "dft_Ex": _peak_err(m.dft("Ex"), acc["Ex"]), "dft_Hy": _peak_err(m.dft("Hy"), acc["Hy"])}
     del g, m, o
     torch.cuda.empty_cache()
@@ -941,8 +949,14 @@ def run_fp64_error_leg(args):
         if ref is None:
             ref = ({f: t.clone() for f, t in cur.items()}, dft)
         else:
+            from opencl_fdtd_solver_b200 import ETA0
+
+            e_peak = max(float(ref[0][f].abs().max()) for f in ("Ex", "Ey", "Ez"))
             for f, t in cur.items():
-                errs[f] = float((t - ref[0][f]).abs().max() / ref[0][f].abs().max())
+                d = float((t - ref[0][f]).abs().max())
+                errs[f] = d / float(ref[0][f].abs().max())
+                if f[0] == "H":
+                    errs[f + "_over_eta0_E_peak"] = ETA0 * d / e_peak
             errs["dft_Ex"] = _peak_err(dft, ref[1])
         del gr, mr, cur
         torch.cuda.empty_cache()
