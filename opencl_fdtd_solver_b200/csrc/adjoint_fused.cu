@@ -12,8 +12,10 @@
 //   Ēz' = Ēz + (((−v_x[j−1]) − (−v_x)) + (v_y[i−1] − v_y))
 // which are the fast-path expressions of adj_h_cell / adj_e_cell operand for
 // operand, so with --fmad=false every cell equals the per-cell kernels bit for
-// bit.  The gradient Σ Ē·(E^{n+1} − E^n) of the cells in the gradient box is
-// accumulated in the H̄ pass, from Ē before the step, as adj_h_cell does.
+// bit.  The gradient Σ Ē·(E^{n+1} − E^n) of the gradient-box cells the march
+// updates is accumulated by k_adj_grad_box on the side stream (its dependent
+// global reads stalled the march when done inside it), from Ē before the step,
+// with the operations of adj_h_cell.
 //
 // Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'):
 //   side stream (slot 1):  k_adj_shell_H on the cells outside HB = [npml,
@@ -101,7 +103,6 @@ struct AdjMarch {
     T ik, wk;  // 1/dl and dtm/dl as the per-cell kernels round them
     T *Eo[3];
     T *Ho[3];
-    AdjGrad<T> gb;
 };
 
 __device__ __forceinline__ bool adj_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
@@ -132,6 +133,22 @@ __device__ __forceinline__ void march_grad(const AdjGrad<T> &gb, int i, int j, i
         const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
         gb.g[q] = gb.g[q] + (double)ev[c] * de;
     }
+}
+
+// G += Ē·(E^{n+1} − E^n) over the gradient-box cells of the box [lo, hi) (the
+// gradient box clipped to HB, whose cells the interior march updates): one
+// thread per cell, Ē read before the step (the fused step writes Ē' elsewhere).
+template <typename T>
+__global__ void k_adj_grad_box(const T *E0, const T *E1, const T *E2, int ny, int nz,
+                               AdjGrad<T> gb, int3 lo, int3 ext) {
+    const int64_t n = (int64_t)ext.x * ext.y * ext.z;
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int k = lo.z + (int)(q % ext.z);
+    const int64_t t = q / ext.z;
+    const int j = lo.y + (int)(t % ext.y), i = lo.x + (int)(t / ext.y);
+    const int64_t idx = ((int64_t)i * ny + j) * nz + k;
+    march_grad<T>(gb, i, j, k, E0[idx], E1[idx], E2[idx]);
 }
 
 template <typename T, int NSTAGE, int GG>
@@ -287,12 +304,6 @@ __global__ void __launch_bounds__(A_NTHREADS, 2)
                             m.Ho[1][gi + v] = hy[v];
                             m.Ho[2][gi + v] = hz[v];
                         }
-                }
-                if (m.gb.active && p >= m.gb.lo[0] && p < m.gb.hi[0] && j >= m.gb.lo[1] &&
-                    j < m.gb.hi[1]) {
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        if (kH[v]) march_grad<T>(m.gb, p, j, kb + v, ex0[v], ey0[v], ez0[v]);
                 }
             }
         } else if (doE) {
@@ -452,7 +463,6 @@ cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjGrad<T> &gb, const
         m.Eo[c] = out.E[c];
         m.Ho[c] = out.H[c];
     }
-    m.gb = gb;
     dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
     cudaError_t e = cudaFuncSetAttribute(k_adj_interior<T, A_NSTAGE, GG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -516,6 +526,25 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
     if ((e = cudaEventRecord(side->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(side->s, side->fork, 0)) != cudaSuccess) return e;
     const bool split = split_shell_e();
+    if (gb.active) {
+        // the gradient of the cells the march updates, off its critical path
+        int lo[3], hi[3];
+        bool any = true;
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = gb.lo[d] > hb.lo[d] ? gb.lo[d] : hb.lo[d];
+            hi[d] = gb.hi[d] < hb.hi[d] ? gb.hi[d] : hb.hi[d];
+            any = any && hi[d] > lo[d];
+        }
+        if (any) {
+            const int3 l = make_int3(lo[0], lo[1], lo[2]);
+            const int3 x = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+            const int64_t cells = (int64_t)x.x * x.y * x.z;
+            k_adj_grad_box<T><<<(unsigned)((cells + 255) / 256), 256, 0, side->s>>>(
+                a.E[0], a.E[1], a.E[2], a.ny, a.nz, gb, l, x);
+            count_launches(1);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
     e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, side->s);
     if (e == cudaSuccess && split) e = launch_adjoint_shell_E<T>(a, out, all, rb, side->s);
     cudaError_t e2 = cudaEventRecord(side->join, side->s);

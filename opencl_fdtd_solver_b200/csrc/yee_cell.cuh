@@ -97,44 +97,36 @@ __device__ __forceinline__ void h_cell(bool interior, int i, int j, int k, int n
         hz = hz - dtm_dl * (d.yx - d.xy);
         return;
     }
-    // psi order: 0 Hx_y, 1 Hx_z, 2 Hy_x, 3 Hy_z, 4 Hz_x, 5 Hz_y.  The ψ reads of
-    // all three axes are issued together, before any of them is used: a cell
-    // outside an axis' slab reads a harmless valid address instead (its value
-    // is discarded), so no load waits behind a branch.
-    const bool inx = npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi);
-    const bool iny = in_slab(j, ny, npml), inz = in_slab(k, nz, npml);
-    const int64_t sx = inx ? psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi) : 0;
-    const int64_t sy = iny ? psi_y_index(i, j, k, ny, nz, npml) : 0;
-    const int64_t sz = inz ? psi_z_index(i, j, k, ny, nz, npml) : 0;
-    const T *dummy = cp.b[0];
-    const T rx2 = *(inx ? psi_rd[2] + sx : dummy), rx4 = *(inx ? psi_rd[4] + sx : dummy);
-    const T ry0 = *(iny ? psi_rd[0] + sy : dummy), ry5 = *(iny ? psi_rd[5] + sy : dummy);
-    const T rz1 = *(inz ? psi_rd[1] + sz : dummy), rz3 = *(inz ? psi_rd[3] + sz : dummy);
-    const T bx = cp.b[0][i], cx = cp.c[0][i], by = cp.b[1][j], cy = cp.c[1][j];
-    const T bz = cp.b[2][k], cz = cp.c[2][k];
+    // psi order: 0 Hx_y, 1 Hx_z, 2 Hy_x, 3 Hy_z, 4 Hz_x, 5 Hz_y
     T p_hx_y = T(0), p_hx_z = T(0), p_hy_x = T(0), p_hy_z = T(0), p_hz_x = T(0), p_hz_y = T(0);
-    if (inx) {
-        p_hy_x = bx * rx2 + cx * d.zx;
-        p_hz_x = bx * rx4 + cx * d.yx;
+    if (npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi)) {
+        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi);
+        const T b = cp.b[0][i], c = cp.c[0][i];
+        p_hy_x = b * psi_rd[2][s] + c * d.zx;
+        p_hz_x = b * psi_rd[4][s] + c * d.yx;
         if (WRITE_PSI) {
-            psi_wr[2][sx] = p_hy_x;
-            psi_wr[4][sx] = p_hz_x;
+            psi_wr[2][s] = p_hy_x;
+            psi_wr[4][s] = p_hz_x;
         }
     }
-    if (iny) {
-        p_hx_y = by * ry0 + cy * d.zy;
-        p_hz_y = by * ry5 + cy * d.xy;
+    if (in_slab(j, ny, npml)) {
+        const int64_t s = psi_y_index(i, j, k, ny, nz, npml);
+        const T b = cp.b[1][j], c = cp.c[1][j];
+        p_hx_y = b * psi_rd[0][s] + c * d.zy;
+        p_hz_y = b * psi_rd[5][s] + c * d.xy;
         if (WRITE_PSI) {
-            psi_wr[0][sy] = p_hx_y;
-            psi_wr[5][sy] = p_hz_y;
+            psi_wr[0][s] = p_hx_y;
+            psi_wr[5][s] = p_hz_y;
         }
     }
-    if (inz) {
-        p_hx_z = bz * rz1 + cz * d.yz;
-        p_hy_z = bz * rz3 + cz * d.xz;
+    if (in_slab(k, nz, npml)) {
+        const int64_t s = psi_z_index(i, j, k, ny, nz, npml);
+        const T b = cp.b[2][k], c = cp.c[2][k];
+        p_hx_z = b * psi_rd[1][s] + c * d.yz;
+        p_hy_z = b * psi_rd[3][s] + c * d.xz;
         if (WRITE_PSI) {
-            psi_wr[1][sz] = p_hx_z;
-            psi_wr[3][sz] = p_hy_z;
+            psi_wr[1][s] = p_hx_z;
+            psi_wr[3][s] = p_hy_z;
         }
     }
     const T ikx = cp.ik[0][i], iky = cp.ik[1][j], ikz = cp.ik[2][k];
@@ -163,37 +155,31 @@ __device__ __forceinline__ void e_cell(bool interior, int i, int j, int k, int n
         ez = (LOSSY ? caz * ez : ez) + cez * inv_dl * (d.yx - d.xy);
         return;
     }
-    // psi order: 0 Ex_y, 1 Ex_z, 2 Ey_x, 3 Ey_z, 4 Ez_x, 5 Ez_y; ψ reads issued
-    // together as in h_cell
-    const bool inx = npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi);
-    const bool iny = in_slab(j, ny, npml), inz = in_slab(k, nz, npml);
-    const int64_t sx = inx ? psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi) : 0;
-    const int64_t sy = iny ? psi_y_index(i, j, k, ny, nz, npml) : 0;
-    const int64_t sz = inz ? psi_z_index(i, j, k, ny, nz, npml) : 0;
-    const T *dummy = cp.b[0];
-    const T rx2 = *(inx ? psi_e[2] + sx : dummy), rx4 = *(inx ? psi_e[4] + sx : dummy);
-    const T ry0 = *(iny ? psi_e[0] + sy : dummy), ry5 = *(iny ? psi_e[5] + sy : dummy);
-    const T rz1 = *(inz ? psi_e[1] + sz : dummy), rz3 = *(inz ? psi_e[3] + sz : dummy);
-    const T bx = cp.b[0][i], cx = cp.c[0][i], by = cp.b[1][j], cy = cp.c[1][j];
-    const T bz = cp.b[2][k], cz = cp.c[2][k];
+    // psi order: 0 Ex_y, 1 Ex_z, 2 Ey_x, 3 Ey_z, 4 Ez_x, 5 Ez_y
     T p_ex_y = T(0), p_ex_z = T(0), p_ey_x = T(0), p_ey_z = T(0), p_ez_x = T(0), p_ez_y = T(0);
-    if (inx) {
-        p_ey_x = bx * rx2 + cx * d.zx;
-        p_ez_x = bx * rx4 + cx * d.yx;
-        psi_e[2][sx] = p_ey_x;
-        psi_e[4][sx] = p_ez_x;
+    if (npml > 0 && in_slab(i, nx, xb.pml_lo, xb.pml_hi)) {
+        const int64_t s = psi_x_index(i, j, k, nx, ny, nz, xb.pml_lo, xb.pml_hi);
+        const T b = cp.b[0][i], c = cp.c[0][i];
+        p_ey_x = b * psi_e[2][s] + c * d.zx;
+        p_ez_x = b * psi_e[4][s] + c * d.yx;
+        psi_e[2][s] = p_ey_x;
+        psi_e[4][s] = p_ez_x;
     }
-    if (iny) {
-        p_ex_y = by * ry0 + cy * d.zy;
-        p_ez_y = by * ry5 + cy * d.xy;
-        psi_e[0][sy] = p_ex_y;
-        psi_e[5][sy] = p_ez_y;
+    if (in_slab(j, ny, npml)) {
+        const int64_t s = psi_y_index(i, j, k, ny, nz, npml);
+        const T b = cp.b[1][j], c = cp.c[1][j];
+        p_ex_y = b * psi_e[0][s] + c * d.zy;
+        p_ez_y = b * psi_e[5][s] + c * d.xy;
+        psi_e[0][s] = p_ex_y;
+        psi_e[5][s] = p_ez_y;
     }
-    if (inz) {
-        p_ex_z = bz * rz1 + cz * d.yz;
-        p_ey_z = bz * rz3 + cz * d.xz;
-        psi_e[1][sz] = p_ex_z;
-        psi_e[3][sz] = p_ey_z;
+    if (in_slab(k, nz, npml)) {
+        const int64_t s = psi_z_index(i, j, k, ny, nz, npml);
+        const T b = cp.b[2][k], c = cp.c[2][k];
+        p_ex_z = b * psi_e[1][s] + c * d.yz;
+        p_ey_z = b * psi_e[3][s] + c * d.xz;
+        psi_e[1][s] = p_ex_z;
+        psi_e[3][s] = p_ey_z;
     }
     const T ikx = cp.ik[0][i], iky = cp.ik[1][j], ikz = cp.ik[2][k];
     ex = (LOSSY ? cax * ex : ex) + cex * (d.zy * iky + p_ex_y - d.yz * ikz - p_ex_z);
