@@ -13,19 +13,16 @@
 // which are the fast-path expressions of adj_h_cell / adj_e_cell operand for
 // operand, so with --fmad=false every cell equals the per-cell kernels bit for
 // bit.  The gradient Σ Ē·(E^{n+1} − E^n) of the gradient-box cells the march
-// updates is accumulated by k_adj_grad_box on the side stream (its dependent
-// global reads stalled the march when done inside it), from Ē before the step,
-// with the operations of adj_h_cell.
+// updates is accumulated by k_adj_grad_box (its dependent global reads stalled
+// the march when done inside it: 98 against 29 µs at 160 x 160 x 96), from Ē
+// before the step, with the operations of adj_h_cell.
 //
-// Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'):
-//   side stream (slot 1):  k_adj_shell_H on the cells outside HB = [npml,
-//                          N-npml-1)^3
-//   caller's stream:       k_adj_interior: H̄' on HB, Ē' on EB = [npml+1, N-npml-1)^3
-//   after the join:        k_adj_shell_E on the cells outside EB, then the
-//                          objective's seed on Ē' (k_adj_seed), in the order
-//                          adj_e_cell adds it.  (With the forward step's split
-//                          knob, the Ē cells outside R = [npml, N-npml)^3 run on
-//                          the side stream instead.)
+// Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'), on
+// the caller's stream: k_adj_grad_box (the gradient of the cells the march
+// updates), k_adj_shell_H on the cells outside HB = [npml, N-npml-1)^3,
+// k_adj_interior (H̄' on HB, Ē' on EB = [npml+1, N-npml-1)^3), k_adj_shell_E on
+// the cells outside EB, then the objective's seed on Ē' (k_adj_seed), in the
+// order adj_e_cell adds it.
 //
 // Interior kernel: each CTA owns a (TJ x TK) tile of (j, k) and marches along i
 // over a chunk of planes.  Plane p arrives by TMA (cp.async.bulk.tensor 3-D
@@ -55,7 +52,6 @@ namespace fdtd {
 
 unsigned interior_wait_polls();
 int interior_chunks(int tiles, int nplanes, int sms);
-bool split_shell_e();
 
 namespace {
 
@@ -509,25 +505,21 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
             e = launch_adjoint_seed<T>(a.nx, a.ny, a.nz, out.E, sd, st);
         return e;
     }
-    ShellBox hb, eb, rb, all;
+    ShellBox hb, eb, all;
     for (int d = 0; d < 3; ++d) {
         hb.lo[d] = a.npml;
         hb.hi[d] = n[d] - a.npml - 1;
         eb.lo[d] = a.npml + 1;
         eb.hi[d] = n[d] - a.npml - 1;
-        rb.lo[d] = a.npml;
-        rb.hi[d] = n[d] - a.npml;
         all.lo[d] = 0;
         all.hi[d] = n[d];
     }
-    SideStream *side = nullptr;
-    cudaError_t e = side_stream(&side, 1);
-    if (e != cudaSuccess) return e;
-    if ((e = cudaEventRecord(side->fork, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(side->s, side->fork, 0)) != cudaSuccess) return e;
-    const bool split = split_shell_e();
+    // all launches on the caller's stream, in this order: the gradient of the
+    // march's cells, shell H̄, the march, shell Ē, the seed.  (On a side stream
+    // beside the march the shell kernels were starved and the step took 155
+    // against 123 µs of serial kernel time at 160 x 160 x 96.)
+    cudaError_t e = cudaSuccess;
     if (gb.active) {
-        // the gradient of the cells the march updates, off its critical path
         int lo[3], hi[3];
         bool any = true;
         for (int d = 0; d < 3; ++d) {
@@ -539,22 +531,17 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
             const int3 l = make_int3(lo[0], lo[1], lo[2]);
             const int3 x = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
             const int64_t cells = (int64_t)x.x * x.y * x.z;
-            k_adj_grad_box<T><<<(unsigned)((cells + 255) / 256), 256, 0, side->s>>>(
+            k_adj_grad_box<T><<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(
                 a.E[0], a.E[1], a.E[2], a.ny, a.nz, gb, l, x);
             count_launches(1);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
     }
-    e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, side->s);
-    if (e == cudaSuccess && split) e = launch_adjoint_shell_E<T>(a, out, all, rb, side->s);
-    cudaError_t e2 = cudaEventRecord(side->join, side->s);
-    if (e == cudaSuccess) e = e2;
+    e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, st);
     if (e == cudaSuccess)
         e = gsel == 8 ? launch_adj_interior<T, 8>(a, gb, out, maps, hb, st)
                       : launch_adj_interior<T, 16>(a, gb, out, maps, hb, st);
-    e2 = cudaStreamWaitEvent(st, side->join, 0);
-    if (e == cudaSuccess) e = e2;
-    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, split ? rb : all, eb, st);
+    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, all, eb, st);
     if (e == cudaSuccess && sd.active)
         e = launch_adjoint_seed<T>(a.nx, a.ny, a.nz, out.E, sd, st);
     return e;
