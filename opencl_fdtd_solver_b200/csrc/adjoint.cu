@@ -102,51 +102,6 @@ __device__ __forceinline__ T h_pair(const AdjArgs<T> &a, int i, int j, int k, T 
     return g;
 }
 
-// Objective seed for E cell (i, j, k): Ē_c += Σ_f Re(seed)·Re(phase) + Im(seed)·Im(phase).
-template <typename T>
-__device__ __forceinline__ void add_seed(const AdjSeed &sd, int i, int j, int k, T &ex, T &ey,
-                                         T &ez) {
-    const int w = sd.axis == 0 ? i : (sd.axis == 1 ? j : k);
-    if (w != sd.index) return;
-    const int pa = sd.axis == 0 ? j : i;
-    const int pb = sd.axis == 2 ? j : k;
-    if (pa < sd.a0 || pa >= sd.a1 || pb < sd.b0 || pb >= sd.b1) return;
-    const int64_t np = (int64_t)(sd.a1 - sd.a0) * (sd.b1 - sd.b0);
-    const int64_t loc = (int64_t)(pa - sd.a0) * (sd.b1 - sd.b0) + (pb - sd.b0);
-    int slot = 0;
-    for (int c = 0; c < 3; ++c) {
-        if (!(sd.comp_mask & (1 << c))) continue;
-        double acc = 0.0;
-        for (int f = 0; f < sd.nfreq; ++f) {
-            const double *s = sd.seed + 2 * (((int64_t)slot * sd.nfreq + f) * np + loc);
-            acc = acc + (s[0] * sd.phase[2 * f] + s[1] * sd.phase[2 * f + 1]);
-        }
-        if (c == 0) ex = ex + (T)acc;
-        if (c == 1) ey = ey + (T)acc;
-        if (c == 2) ez = ez + (T)acc;
-        ++slot;
-    }
-}
-
-// G_c += Ē_c·(E_c^{n+1} − E_c^n) for a cell of the gradient box.
-template <typename T>
-__device__ __forceinline__ void adj_grad_cell(const AdjGrad<T> &gb, int i, int j, int k, T ex,
-                                              T ey, T ez) {
-    if (i < gb.lo[0] || i >= gb.hi[0] || j < gb.lo[1] || j >= gb.hi[1] || k < gb.lo[2] ||
-        k >= gb.hi[2])
-        return;
-    const int by = gb.hi[1] - gb.lo[1], bz = gb.hi[2] - gb.lo[2];
-    const int64_t nb = (int64_t)(gb.hi[0] - gb.lo[0]) * by * bz;
-    const int64_t loc = ((int64_t)(i - gb.lo[0]) * by + (j - gb.lo[1])) * bz + (k - gb.lo[2]);
-    const T ev[3] = {ex, ey, ez};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const int64_t q = c * nb + loc;
-        const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
-        gb.g[q] = gb.g[q] + (double)ev[c] * de;
-    }
-}
-
 // Transposed E update of cell (i, j, k): H̄ += B^T ḡ(Ē, P_E) into Hout (Hout
 // == a.H updates in place), P_E advanced, gradient accumulated.
 template <typename T>
@@ -295,22 +250,35 @@ __global__ void __launch_bounds__(ADJ_TK *ADJ_TJ)
 }
 
 // Shell reverse half steps: the cells of box o outside box b (shell_plan.cuh).
+// Threads beyond the shell's cells accumulate the gradient of the box gx (the
+// gradient box clipped to the interior march's box, whose cells the march does
+// not accumulate), with the operations of adj_grad_cell.
 template <typename T>
 __global__ void __launch_bounds__(SHELL_THREADS)
-    k_adj_shell_H(AdjArgs<T> a, AdjGrad<T> gb, AdjOut<T> out, ShellPlan sp) {
+    k_adj_shell_H(AdjArgs<T> a, AdjGrad<T> gb, AdjOut<T> out, ShellPlan sp, ShellBox gx) {
+    const unsigned t = blockIdx.x * SHELL_THREADS + threadIdx.x;
     int i, j, k;
-    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
-    adj_h_cell<T>(a, gb, i, j, k, out.H);
+    if (shell_cell(t, sp, i, j, k)) {
+        adj_h_cell<T>(a, gb, i, j, k, out.H);
+        return;
+    }
+    const unsigned q = t - (sp.nA + sp.nB + sp.nC);
+    const unsigned ez = (unsigned)(gx.hi[2] - gx.lo[2]), ey = (unsigned)(gx.hi[1] - gx.lo[1]);
+    const unsigned ng = (unsigned)(gx.hi[0] - gx.lo[0]) * ey * ez;
+    if (!gb.active || q >= ng) return;
+    k = gx.lo[2] + (int)(q % ez);
+    j = gx.lo[1] + (int)((q / ez) % ey);
+    i = gx.lo[0] + (int)(q / (ez * ey));
+    const int64_t idx = ((int64_t)i * a.ny + j) * a.nz + k;
+    adj_grad_cell(gb, i, j, k, a.E[0][idx], a.E[1][idx], a.E[2][idx]);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(SHELL_THREADS)
-    k_adj_shell_E(AdjArgs<T> a, AdjOut<T> out, ShellPlan sp) {
+    k_adj_shell_E(AdjArgs<T> a, AdjSeed sd, AdjOut<T> out, ShellPlan sp) {
     int i, j, k;
     if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
-    AdjSeed none;
-    none.active = 0;
-    adj_e_cell<T>(a, none, i, j, k, out.H, out.E);
+    adj_e_cell<T>(a, sd, i, j, k, out.H, out.E);
 }
 
 // Seed only (before the first reverse step): one thread per patch cell.
@@ -376,24 +344,30 @@ cudaError_t launch_adjoint_grid(const AdjArgs<T> &a, const AdjGrad<T> &gb, const
 
 template <typename T>
 cudaError_t launch_adjoint_shell_H(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjOut<T> &out,
-                                   const ShellBox &o, const ShellBox &b, cudaStream_t st) {
+                                   const ShellBox &o, const ShellBox &b, const ShellBox &gx,
+                                   cudaStream_t st) {
     if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
     const ShellPlan sp = make_plan(o, b);
-    const unsigned nb = shell_blocks(sp);
+    int64_t ng = 1;
+    for (int d = 0; d < 3; ++d) ng *= (gx.hi[d] > gx.lo[d]) ? gx.hi[d] - gx.lo[d] : 0;
+    if (!gb.active) ng = 0;
+    const uint64_t n = (uint64_t)sp.nA + sp.nB + sp.nC + (uint64_t)ng;
+    if (n + SHELL_THREADS >= 0xffffffffull) return cudaErrorInvalidConfiguration;
+    const unsigned nb = (unsigned)((n + SHELL_THREADS - 1) / SHELL_THREADS);
     if (nb == 0) return cudaSuccess;
-    k_adj_shell_H<T><<<nb, SHELL_THREADS, 0, st>>>(a, gb, out, sp);
+    k_adj_shell_H<T><<<nb, SHELL_THREADS, 0, st>>>(a, gb, out, sp, gx);
     count_launches(1);
     return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_adjoint_shell_E(const AdjArgs<T> &a, const AdjOut<T> &out, const ShellBox &o,
-                                   const ShellBox &b, cudaStream_t st) {
+cudaError_t launch_adjoint_shell_E(const AdjArgs<T> &a, const AdjSeed &sd, const AdjOut<T> &out,
+                                   const ShellBox &o, const ShellBox &b, cudaStream_t st) {
     if (!plan_fits(o)) return cudaErrorInvalidConfiguration;
     const ShellPlan sp = make_plan(o, b);
     const unsigned nb = shell_blocks(sp);
     if (nb == 0) return cudaSuccess;
-    k_adj_shell_E<T><<<nb, SHELL_THREADS, 0, st>>>(a, out, sp);
+    k_adj_shell_E<T><<<nb, SHELL_THREADS, 0, st>>>(a, sd, out, sp);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -435,10 +409,11 @@ template cudaError_t launch_adjoint_step<double>(const AdjArgs<double> &,
                                                 cudaStream_t);                               \
     template cudaError_t launch_adjoint_shell_H<T>(const AdjArgs<T> &, const AdjGrad<T> &,   \
                                                    const AdjOut<T> &, const ShellBox &,      \
-                                                   const ShellBox &, cudaStream_t);          \
-    template cudaError_t launch_adjoint_shell_E<T>(const AdjArgs<T> &, const AdjOut<T> &,    \
                                                    const ShellBox &, const ShellBox &,       \
-                                                   cudaStream_t);
+                                                   cudaStream_t);                            \
+    template cudaError_t launch_adjoint_shell_E<T>(const AdjArgs<T> &, const AdjSeed &,      \
+                                                   const AdjOut<T> &, const ShellBox &,      \
+                                                   const ShellBox &, cudaStream_t);
 FDTD_ADJ_INST(float)
 FDTD_ADJ_INST(double)
 #undef FDTD_ADJ_INST

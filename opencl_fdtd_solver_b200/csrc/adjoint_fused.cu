@@ -13,16 +13,16 @@
 // which are the fast-path expressions of adj_h_cell / adj_e_cell operand for
 // operand, so with --fmad=false every cell equals the per-cell kernels bit for
 // bit.  The gradient Σ Ē·(E^{n+1} − E^n) of the gradient-box cells the march
-// updates is accumulated by k_adj_grad_box (its dependent global reads stalled
-// the march when done inside it: 98 against 29 µs at 160 x 160 x 96), from Ē
-// before the step, with the operations of adj_h_cell.
+// updates is accumulated by extra threads of the shell-H̄ launch (its dependent
+// global reads stalled the march when done inside it: 98 against 29 µs at
+// 160 x 160 x 96), from Ē before the step, with the operations of adj_h_cell.
 //
-// Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'), on
-// the caller's stream: k_adj_grad_box (the gradient of the cells the march
-// updates), k_adj_shell_H on the cells outside HB = [npml, N-npml-1)^3,
-// k_adj_interior (H̄' on HB, Ē' on EB = [npml+1, N-npml-1)^3), k_adj_shell_E on
-// the cells outside EB, then the objective's seed on Ē' (k_adj_seed), in the
-// order adj_e_cell adds it.
+// Schedule of one fused reverse step (reads Ē, H̄, P; writes Ē', H̄', P'), three
+// launches on the caller's stream: k_adj_shell_H on the cells outside HB =
+// [npml, N-npml-1)^3 (extra threads accumulate the gradient of the gradient-box
+// cells inside HB), k_adj_interior (H̄' on HB, Ē' on EB = [npml+1, N-npml-1)^3),
+// k_adj_shell_E on the cells outside EB; the objective's seed is added to Ē' in
+// the last two, in the order adj_e_cell adds it.
 //
 // Interior kernel: each CTA owns a (TJ x TK) tile of (j, k) and marches along i
 // over a chunk of planes.  Plane p arrives by TMA (cp.async.bulk.tensor 3-D
@@ -99,6 +99,7 @@ struct AdjMarch {
     T ik, wk;  // 1/dl and dtm/dl as the per-cell kernels round them
     T *Eo[3];
     T *Ho[3];
+    AdjSeed sd;  // the objective's seed, added to Ē' of its patch cells
 };
 
 __device__ __forceinline__ bool adj_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
@@ -110,41 +111,6 @@ __device__ __forceinline__ bool adj_wait(uint64_t *bar, uint32_t parity, unsigne
     }
     atomicOr(&g_adj_error, 1);
     return false;
-}
-
-// G += Ē·(E^{n+1} − E^n) of one cell of the gradient box (as adj_grad_cell).
-template <typename T>
-__device__ __forceinline__ void march_grad(const AdjGrad<T> &gb, int i, int j, int k, T ex, T ey,
-                                           T ez) {
-    if (i < gb.lo[0] || i >= gb.hi[0] || j < gb.lo[1] || j >= gb.hi[1] || k < gb.lo[2] ||
-        k >= gb.hi[2])
-        return;
-    const int by = gb.hi[1] - gb.lo[1], bz = gb.hi[2] - gb.lo[2];
-    const int64_t nb = (int64_t)(gb.hi[0] - gb.lo[0]) * by * bz;
-    const int64_t loc = ((int64_t)(i - gb.lo[0]) * by + (j - gb.lo[1])) * bz + (k - gb.lo[2]);
-    const T ev[3] = {ex, ey, ez};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const int64_t q = c * nb + loc;
-        const double de = (double)gb.e_next[q] - (double)gb.e_prev[q];
-        gb.g[q] = gb.g[q] + (double)ev[c] * de;
-    }
-}
-
-// G += Ē·(E^{n+1} − E^n) over the gradient-box cells of the box [lo, hi) (the
-// gradient box clipped to HB, whose cells the interior march updates): one
-// thread per cell, Ē read before the step (the fused step writes Ē' elsewhere).
-template <typename T>
-__global__ void k_adj_grad_box(const T *E0, const T *E1, const T *E2, int ny, int nz,
-                               AdjGrad<T> gb, int3 lo, int3 ext) {
-    const int64_t n = (int64_t)ext.x * ext.y * ext.z;
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    const int k = lo.z + (int)(q % ext.z);
-    const int64_t t = q / ext.z;
-    const int j = lo.y + (int)(t % ext.y), i = lo.x + (int)(t / ext.y);
-    const int64_t idx = ((int64_t)i * ny + j) * nz + k;
-    march_grad<T>(gb, i, j, k, E0[idx], E1[idx], E2[idx]);
 }
 
 template <typename T, int NSTAGE, int GG>
@@ -369,6 +335,7 @@ __global__ void __launch_bounds__(A_NTHREADS, 2)
                 ex0[v] = ex0[v] + ((a3p - a3) + (a5p - a5));
                 ey0[v] = ey0[v] + ((a1p - a1) + (a4p - a4));
                 ez0[v] = ez0[v] + ((a0p - a0) + (a2p - a2));
+                if (m.sd.active && kE[v]) add_seed<T>(m.sd, p, j, kb + v, ex0[v], ey0[v], ez0[v]);
             }
             const int64_t gi = (int64_t)p * sx + (int64_t)j * nz + kb;
             if (allE) {
@@ -426,7 +393,7 @@ bool adj_maps(const AdjArgs<T> &a, AdjMaps &maps) {
 }
 
 template <typename T, int GG>
-cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjGrad<T> &gb, const AdjOut<T> &out,
+cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjSeed &sd, const AdjOut<T> &out,
                                 const AdjMaps &maps, const ShellBox &hb, cudaStream_t st) {
     using L = ATile<T, GG>;
     AdjBox bx;
@@ -459,6 +426,7 @@ cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjGrad<T> &gb, const
         m.Eo[c] = out.E[c];
         m.Ho[c] = out.H[c];
     }
+    m.sd = sd;
     dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
     cudaError_t e = cudaFuncSetAttribute(k_adj_interior<T, A_NSTAGE, GG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -514,36 +482,22 @@ cudaError_t launch_adjoint_step_fused(const AdjArgs<T> &a, const AdjGrad<T> &gb,
         all.lo[d] = 0;
         all.hi[d] = n[d];
     }
-    // all launches on the caller's stream, in this order: the gradient of the
-    // march's cells, shell H̄, the march, shell Ē, the seed.  (On a side stream
-    // beside the march the shell kernels were starved and the step took 155
-    // against 123 µs of serial kernel time at 160 x 160 x 96.)
-    cudaError_t e = cudaSuccess;
-    if (gb.active) {
-        int lo[3], hi[3];
-        bool any = true;
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = gb.lo[d] > hb.lo[d] ? gb.lo[d] : hb.lo[d];
-            hi[d] = gb.hi[d] < hb.hi[d] ? gb.hi[d] : hb.hi[d];
-            any = any && hi[d] > lo[d];
-        }
-        if (any) {
-            const int3 l = make_int3(lo[0], lo[1], lo[2]);
-            const int3 x = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
-            const int64_t cells = (int64_t)x.x * x.y * x.z;
-            k_adj_grad_box<T><<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(
-                a.E[0], a.E[1], a.E[2], a.ny, a.nz, gb, l, x);
-            count_launches(1);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
+    // three launches on the caller's stream: shell H̄ (whose extra threads also
+    // accumulate the gradient of the march's cells), the march, shell Ē; the
+    // seed is added in the Ē epilogues of the last two.  (On a side stream
+    // beside the march the shell kernels were starved; as separate launches the
+    // gradient and seed kernels added gaps between short dependent kernels.)
+    ShellBox gx;
+    for (int d = 0; d < 3; ++d) {
+        gx.lo[d] = gb.lo[d] > hb.lo[d] ? gb.lo[d] : hb.lo[d];
+        gx.hi[d] = gb.hi[d] < hb.hi[d] ? gb.hi[d] : hb.hi[d];
+        if (!gb.active || gx.hi[d] < gx.lo[d]) gx.hi[d] = gx.lo[d];
     }
-    e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, st);
+    cudaError_t e = launch_adjoint_shell_H<T>(a, gb, out, all, hb, gx, st);
     if (e == cudaSuccess)
-        e = gsel == 8 ? launch_adj_interior<T, 8>(a, gb, out, maps, hb, st)
-                      : launch_adj_interior<T, 16>(a, gb, out, maps, hb, st);
-    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, out, all, eb, st);
-    if (e == cudaSuccess && sd.active)
-        e = launch_adjoint_seed<T>(a.nx, a.ny, a.nz, out.E, sd, st);
+        e = gsel == 8 ? launch_adj_interior<T, 8>(a, sd, out, maps, hb, st)
+                      : launch_adj_interior<T, 16>(a, sd, out, maps, hb, st);
+    if (e == cudaSuccess) e = launch_adjoint_shell_E<T>(a, sd, out, all, eb, st);
     return e;
 }
 
