@@ -28,8 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", str(ROOT / "include")]
 # Files whose arithmetic must round like the oracle.
-NO_FMA = {"yee_split.cu", "yee_fused.cu", "yee_shell.cu", "dft.cu", "adjoint.cu", "adjoint_fused.cu",
-          "materials.cu"}
+NO_FMA = {"yee_split.cu", "yee_fused.cu", "yee_shell.cu", "yee_face.cu", "dft.cu", "adjoint.cu",
+          "adjoint_fused.cu", "materials.cu"}
 
 
 def nvcc() -> str:

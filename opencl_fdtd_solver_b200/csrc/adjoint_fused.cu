@@ -50,7 +50,6 @@
 
 namespace fdtd {
 
-unsigned interior_wait_polls();
 int interior_chunks(int tiles, int nplanes, int sms);
 
 namespace {

@@ -116,6 +116,61 @@ inline unsigned shell_blocks(const ShellPlan &s) {
     return (unsigned)((n + SHELL_THREADS - 1) / SHELL_THREADS);
 }
 
+// Enumeration of the cells of up to MAX_PLAN_BOXES disjoint boxes, one flat
+// index per cell (box by box, k fastest), decoded with the same multiply-high
+// divisions.
+constexpr int MAX_PLAN_BOXES = 16;
+struct BoxPlan {
+    int n;
+    ShellBox box[MAX_PLAN_BOXES];
+    unsigned start[MAX_PLAN_BOXES + 1];                      // flat index of each box's first cell
+    FastDiv d_plane[MAX_PLAN_BOXES], d_row[MAX_PLAN_BOXES];  // ey*ez, ez of each box
+};
+
+__device__ __forceinline__ bool box_cell(unsigned t, const BoxPlan &p, int &i, int &j, int &k) {
+    if (t >= p.start[p.n]) return false;
+    int b = 0;
+    while (b + 1 < p.n && t >= p.start[b + 1]) ++b;
+    t -= p.start[b];
+    const unsigned q = fdiv(t, p.d_plane[b]);
+    const unsigned rem = t - q * p.d_plane[b].d;
+    const unsigned r = fdiv(rem, p.d_row[b]);
+    i = p.box[b].lo[0] + (int)q;
+    j = p.box[b].lo[1] + (int)r;
+    k = p.box[b].lo[2] + (int)(rem - r * p.d_row[b].d);
+    return true;
+}
+
+// Appends box [lo, hi) to the plan (empty boxes are skipped); false when the
+// plan is full or the cell count would leave 32 bits.
+inline bool plan_add(BoxPlan &p, int lo0, int hi0, int lo1, int hi1, int lo2, int hi2) {
+    if (hi0 <= lo0 || hi1 <= lo1 || hi2 <= lo2) return true;
+    if (p.n >= MAX_PLAN_BOXES) return false;
+    const uint64_t cells = (uint64_t)(hi0 - lo0) * (hi1 - lo1) * (hi2 - lo2);
+    if ((uint64_t)p.start[p.n] + cells + SHELL_THREADS >= 0xffffffffull) return false;
+    ShellBox &b = p.box[p.n];
+    b.lo[0] = lo0;
+    b.hi[0] = hi0;
+    b.lo[1] = lo1;
+    b.hi[1] = hi1;
+    b.lo[2] = lo2;
+    b.hi[2] = hi2;
+    p.d_plane[p.n] = make_fastdiv((unsigned)((hi1 - lo1) * (hi2 - lo2)));
+    p.d_row[p.n] = make_fastdiv((unsigned)(hi2 - lo2));
+    p.start[p.n + 1] = p.start[p.n] + (unsigned)cells;
+    ++p.n;
+    return true;
+}
+
+inline unsigned plan_blocks(const BoxPlan &p) {
+    return (unsigned)(((uint64_t)p.start[p.n] + SHELL_THREADS - 1) / SHELL_THREADS);
+}
+
+// E^{n+1} of the cells of the plan's boxes (per-cell kernel, yee_shell.cu).
+template <typename T>
+cudaError_t launch_shell_E_boxes(const YeeArgs<T> &a, const BoxPlan &bp, const SourceList &src,
+                                 const PlaneList &pl, cudaStream_t st);
+
 inline bool plan_fits(const ShellBox &o) {
     // every group count and the flat index must fit in 32 bits
     const int64_t ex[3] = {o.hi[0] - o.lo[0], o.hi[1] - o.lo[1], o.hi[2] - o.lo[2]};

@@ -89,10 +89,12 @@ __device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
 
 // 3-D tiled tensor map (x = z-index fastest, y = j, z = i) of an (nx, ny, nz)
 // array of elem-byte values with a box of b0 x b1 x 1, no swizzle, no
-// multicast; cached by (base, shape, elem, box).  False if the driver's encoder
-// is unavailable or rejects the map.
+// multicast; cached by (base, shape, elem, box, promotion).  l2_promote: the L2
+// fetch granularity of the copies in bytes (256, 128, 64; 0 = none, for boxes
+// whose rows are short runs that neighbouring tiles do not share).  False if
+// the driver's encoder is unavailable or rejects the map.
 bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem,
-                     int b0, int b1);
+                     int b0, int b1, int l2_promote = 256);
 
 // A stream of this host thread and device, with events to fork from and join
 // back to a caller's stream.  slot 0 serves the forward step, slot 1 the

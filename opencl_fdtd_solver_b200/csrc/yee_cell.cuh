@@ -141,6 +141,28 @@ struct DH {
     T zy, yz, xz, zx, yx, xy;
 };
 
+// Interior E update (yee_update.cl:145-154): folded ce * (1/dl).
+template <typename T, bool LOSSY>
+__device__ __forceinline__ void e_interior(const DH<T> &d, T inv_dl, T cax, T cay, T caz, T cex,
+                                           T cey, T cez, T &ex, T &ey, T &ez) {
+    ex = (LOSSY ? cax * ex : ex) + cex * inv_dl * (d.zy - d.yz);
+    ey = (LOSSY ? cay * ey : ey) + cey * inv_dl * (d.xz - d.zx);
+    ez = (LOSSY ? caz * ez : ez) + cez * inv_dl * (d.yx - d.xy);
+}
+
+// CPML E update given the six ψ_E terms of the cell (zero on the axes whose
+// slab the cell is not in) and the 1/(kappa*dl) of its three coordinates
+// (yee_update.cl:233-237).
+template <typename T, bool LOSSY>
+__device__ __forceinline__ void e_combine(const DH<T> &d, T ikx, T iky, T ikz, T p_ex_y,
+                                          T p_ex_z, T p_ey_x, T p_ey_z, T p_ez_x, T p_ez_y,
+                                          T cax, T cay, T caz, T cex, T cey, T cez, T &ex,
+                                          T &ey, T &ez) {
+    ex = (LOSSY ? cax * ex : ex) + cex * (d.zy * iky + p_ex_y - d.yz * ikz - p_ex_z);
+    ey = (LOSSY ? cay * ey : ey) + cey * (d.xz * ikz + p_ey_z - d.zx * ikx - p_ey_x);
+    ez = (LOSSY ? caz * ez : ez) + cez * (d.yx * ikx + p_ez_x - d.xy * iky - p_ez_y);
+}
+
 // E update of one cell.  ex/ey/ez enter as E^n (with any sheet injection
 // already added) and leave as E^{n+1}.  psi_e is updated in place.
 template <typename T, bool LOSSY>
@@ -150,9 +172,7 @@ __device__ __forceinline__ void e_cell(bool interior, int i, int j, int k, int n
                                        const Cpml1D<T> &cp, T *const *psi_e, T cax, T cay,
                                        T caz, T cex, T cey, T cez, T &ex, T &ey, T &ez) {
     if (interior) {
-        ex = (LOSSY ? cax * ex : ex) + cex * inv_dl * (d.zy - d.yz);
-        ey = (LOSSY ? cay * ey : ey) + cey * inv_dl * (d.xz - d.zx);
-        ez = (LOSSY ? caz * ez : ez) + cez * inv_dl * (d.yx - d.xy);
+        e_interior<T, LOSSY>(d, inv_dl, cax, cay, caz, cex, cey, cez, ex, ey, ez);
         return;
     }
     // psi order: 0 Ex_y, 1 Ex_z, 2 Ey_x, 3 Ey_z, 4 Ez_x, 5 Ez_y
@@ -181,10 +201,8 @@ __device__ __forceinline__ void e_cell(bool interior, int i, int j, int k, int n
         psi_e[1][s] = p_ex_z;
         psi_e[3][s] = p_ey_z;
     }
-    const T ikx = cp.ik[0][i], iky = cp.ik[1][j], ikz = cp.ik[2][k];
-    ex = (LOSSY ? cax * ex : ex) + cex * (d.zy * iky + p_ex_y - d.yz * ikz - p_ex_z);
-    ey = (LOSSY ? cay * ey : ey) + cey * (d.xz * ikz + p_ey_z - d.zx * ikx - p_ey_x);
-    ez = (LOSSY ? caz * ez : ez) + cez * (d.yx * ikx + p_ez_x - d.xy * iky - p_ez_y);
+    e_combine<T, LOSSY>(d, cp.ik[0][i], cp.ik[1][j], cp.ik[2][k], p_ex_y, p_ex_z, p_ey_x, p_ey_z,
+                        p_ez_x, p_ez_y, cax, cay, caz, cex, cey, cez, ex, ey, ez);
 }
 
 // Pending sheet injections for one launch, passed by value.
@@ -269,6 +287,16 @@ __device__ __forceinline__ void plane_dft_cell(const PlaneList &pl, int i, int j
             ++slot;
         }
     }
+}
+
+// The plane DFTs of one cell, called out of line from the shell kernels.
+// planes points at the kernel's __grid_constant__ parameter, so the call takes
+// no local copy of the descriptor list.
+static __device__ __noinline__ void shell_dft(const PlaneList *planes, int i, int j, int k,
+                                              int nx, int ny, int nz, double ex, double ey,
+                                              double ez, double hx, double hy, double hz) {
+    const double v[6] = {ex, ey, ez, hx, hy, hz};
+    plane_dft_cell(*planes, i, j, k, nx, ny, nz, v);
 }
 
 }  // namespace fdtd

@@ -437,7 +437,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 struct MapKey {
     const void *base;
-    int nx, ny, nz, elem, b0, b1;
+    int nx, ny, nz, elem, b0, b1, promo;
     bool operator==(const MapKey &o) const { return memcmp(this, &o, sizeof(MapKey)) == 0; }
 };
 struct MapKeyHash {
@@ -455,7 +455,7 @@ std::unordered_map<MapKey, CUtensorMap, MapKeyHash> g_maps;
 }  // namespace
 
 bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem,
-                     int b0, int b1) {
+                     int b0, int b1, int l2_promote) {
     MapKey key;
     memset(&key, 0, sizeof(key));
     key.base = base;
@@ -465,6 +465,7 @@ bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz,
     key.elem = elem;
     key.b0 = b0;
     key.b1 = b1;
+    key.promo = l2_promote;
     std::lock_guard<std::mutex> lk(g_map_mu);
     auto it = g_maps.find(key);
     if (it != g_maps.end()) {
@@ -477,10 +478,15 @@ bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz,
     cuuint64_t strides[2] = {(cuuint64_t)nz * elem, (cuuint64_t)ny * nz * elem};
     cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, 1};
     cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapL2promotion promo =
+        l2_promote >= 256   ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+        : l2_promote >= 128 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+        : l2_promote >= 64  ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+                            : CU_TENSOR_MAP_L2_PROMOTION_NONE;
     CUresult r = fn(out, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                     3, const_cast<void *>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
     if (g_maps.size() > 4096) g_maps.clear();
     g_maps.emplace(key, *out);
@@ -596,6 +602,7 @@ struct StepProfiler {
     std::mutex mu;
     bool on = false;
     std::vector<std::array<cudaEvent_t, NEV>> pending;
+    std::vector<bool> dft_last;  // per pending step: the plane DFT ran after shell E
     double ms[NPROF] = {0.0, 0.0, 0.0, 0.0, 0.0};
     int steps = 0;
 };
@@ -604,11 +611,15 @@ StepProfiler g_prof;
 // Waits for the recorded steps, adds their launch times, releases the events.
 cudaError_t prof_flush_locked() {
     cudaError_t err = cudaSuccess;
-    for (auto &ev : g_prof.pending) {
+    for (size_t q = 0; q < g_prof.pending.size(); ++q) {
+        auto &ev = g_prof.pending[q];
         // ev: 0 start, 1 shell H done (side stream), 2 outer shell E done (side),
-        // 3 interior done, 4 joined, 5 plane DFT done, 6 rim E done
+        // 3 interior done, 4 joined, 5 plane DFT done, 6 rim E done; with the
+        // face kernels 5 is shell E done and 6 plane DFT done
         cudaError_t e = cudaEventSynchronize(ev[6]);
-        const int from[NPROF] = {0, 1, 0, 4, 5}, to[NPROF] = {1, 2, 3, 5, 6};
+        const bool late = g_prof.dft_last[q];
+        const int from[NPROF] = {0, 1, 0, late ? 5 : 4, late ? 4 : 5};
+        const int to[NPROF] = {1, 2, 3, late ? 6 : 5, late ? 5 : 6};
         for (int s = 0; s < NPROF && e == cudaSuccess; ++s) {
             float t = 0.f;
             e = cudaEventElapsedTime(&t, ev[from[s]], ev[to[s]]);
@@ -619,6 +630,7 @@ cudaError_t prof_flush_locked() {
         ++g_prof.steps;
     }
     g_prof.pending.clear();
+    g_prof.dft_last.clear();
     return err;
 }
 
@@ -633,9 +645,10 @@ bool prof_begin(std::array<cudaEvent_t, NEV> &ev) {
     return true;
 }
 
-void prof_end(const std::array<cudaEvent_t, NEV> &ev) {
+void prof_end(const std::array<cudaEvent_t, NEV> &ev, bool dft_last) {
     std::lock_guard<std::mutex> lk(g_prof.mu);
     g_prof.pending.push_back(ev);
+    g_prof.dft_last.push_back(dft_last);
     if (g_prof.pending.size() >= 2048) prof_flush_locked();
 }
 }  // namespace
@@ -795,17 +808,28 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
         }
     }
     if (prof) cudaEventRecord(ev[4], st);
-    // plane DFTs of the cells the interior kernel updated
-    if (e == cudaSuccess && use_interior && pl.n) e = launch_plane_dft_box<T>(a, ebox, pl, st);
-    if (prof) cudaEventRecord(ev[5], st);
-    // E of the rim (or of the whole grid without an interior box), or of every
-    // cell outside B' when the outer part did not run on the side stream
-    if (e == cudaSuccess)
-        e = launch_shell_E_region<T>(a, (use_interior && split_shell_e()) ? rbox : all, ebox, src,
-                                     pl, st);
+    const bool faces = use_interior && !split_shell_e() && face_path_ok<T>(a);
+    if (faces) {
+        // shell E through the CPML face marches, then the plane DFTs of every
+        // monitored cell in one pass over the planes
+        if (e == cudaSuccess) e = launch_shell_E_faces<T>(a, src, st, side);
+        if (prof) cudaEventRecord(ev[5], st);
+        if (e == cudaSuccess && pl.n) e = launch_plane_dft_box<T>(a, all, pl, st);
+    } else {
+        // plane DFTs of the cells the interior kernel updated
+        if (e == cudaSuccess && use_interior && pl.n)
+            e = launch_plane_dft_box<T>(a, ebox, pl, st);
+        if (prof) cudaEventRecord(ev[5], st);
+        // E of the rim (or of the whole grid without an interior box), or of
+        // every cell outside B' when the outer part did not run on the side
+        // stream, with the DFTs of those cells
+        if (e == cudaSuccess)
+            e = launch_shell_E_region<T>(a, (use_interior && split_shell_e()) ? rbox : all, ebox,
+                                         src, pl, st);
+    }
     if (prof) {
         cudaEventRecord(ev[6], st);
-        prof_end(ev);
+        prof_end(ev, faces);
     }
     return e;
 }
@@ -823,14 +847,16 @@ void set_interior_wait_polls(int64_t polls) {
                                  : (long long)(polls > (int64_t)WAIT_LIMIT ? WAIT_LIMIT : polls));
 }
 
+// The interior kernel's and the face kernels' flags (one status bit).
 int read_fused_error(int reset) {
+    const int f = read_face_error(reset);
     int v = 0;
     cudaMemcpyFromSymbol(&v, g_fused_error, sizeof(int));
     if (reset) {
         int z = 0;
         cudaMemcpyToSymbol(g_fused_error, &z, sizeof(int));
     }
-    return v;
+    return v | f;
 }
 
 }  // namespace fdtd

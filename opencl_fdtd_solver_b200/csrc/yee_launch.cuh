@@ -48,6 +48,22 @@ template <typename T>
 cudaError_t launch_plane_dft_box(const YeeArgs<T> &a, const ShellBox &b, const PlaneList &pl,
                                  cudaStream_t st);
 
+struct SideStream;
+
+// Shell E of the fused step through the CPML face kernels (yee_face.cu): the
+// six face slabs as TMA plane marches on st, the remaining shell cells by the
+// per-cell kernel on the side stream, joined back to st; no plane DFTs (the
+// caller accumulates the monitored planes afterwards).  face_path_ok: the grid
+// qualifies (whole grid, npml a multiple of 16 bytes of elements, aligned
+// stripes).
+template <typename T>
+bool face_path_ok(const YeeArgs<T> &a);
+template <typename T>
+cudaError_t launch_shell_E_faces(const YeeArgs<T> &a, const SourceList &src, cudaStream_t st,
+                                 SideStream *side);
+int read_face_error(int reset);
+unsigned interior_wait_polls();
+
 template <typename T>
 cudaError_t launch_update_H(const YeeArgs<T> &a, cudaStream_t st);
 template <typename T>

@@ -59,21 +59,13 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     a.H_next[2][idx] = hz;
 }
 
-// planes points at the kernel's __grid_constant__ parameter, so the call takes
-// no local copy of the descriptor list.
-__device__ __noinline__ void shell_dft(const PlaneList *planes, int i, int j, int k, int nx,
-                                       int ny, int nz, double ex, double ey, double ez,
-                                       double hx, double hy, double hz) {
-    const double v[6] = {ex, ey, ez, hx, hy, hz};
-    plane_dft_cell(*planes, i, j, k, nx, ny, nz, v);
-}
-
+// E^{n+1} of cell (i, j, k) from H_next, E, ψ_E in place, with its sheet
+// injections and plane DFTs.  planes is the kernel's __grid_constant__
+// parameter.
 template <typename T, bool LOSSY>
-__global__ void __launch_bounds__(SHELL_THREADS)
-    k_shell_E(YeeArgs<T> a, ShellPlan sp, SourceList src, const __grid_constant__ PlaneList planes) {
+__device__ __forceinline__ void shell_E_cell(const YeeArgs<T> &a, int i, int j, int k,
+                                             const SourceList &src, const PlaneList &planes) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, npml = a.npml;
-    int i, j, k;
-    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
     const int64_t sx = (int64_t)ny * nz, sy = nz;
     const int64_t idx = (int64_t)i * sx + (int64_t)j * sy + k;
     const T *Hx = a.H_next[0], *Hy = a.H_next[1], *Hz = a.H_next[2];
@@ -104,6 +96,25 @@ __global__ void __launch_bounds__(SHELL_THREADS)
     if (planes.n && plane_any_hit(planes, i, j, k))
         shell_dft(&planes, i, j, k, nx, ny, nz, (double)ex, (double)ey, (double)ez, (double)hx0,
                   (double)hy0, (double)hz0);
+}
+
+template <typename T, bool LOSSY>
+__global__ void __launch_bounds__(SHELL_THREADS)
+    k_shell_E(YeeArgs<T> a, ShellPlan sp, SourceList src, const __grid_constant__ PlaneList planes) {
+    int i, j, k;
+    if (!shell_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, sp, i, j, k)) return;
+    shell_E_cell<T, LOSSY>(a, i, j, k, src, planes);
+}
+
+// The same per-cell E update over the cells of a list of boxes (the shell E
+// cells the CPML face kernels do not take: edges, corners and a rim row).
+template <typename T, bool LOSSY>
+__global__ void __launch_bounds__(SHELL_THREADS)
+    k_shell_E_boxes(YeeArgs<T> a, const __grid_constant__ BoxPlan bp, SourceList src,
+                    const __grid_constant__ PlaneList planes) {
+    int i, j, k;
+    if (!box_cell(blockIdx.x * SHELL_THREADS + threadIdx.x, bp, i, j, k)) return;
+    shell_E_cell<T, LOSSY>(a, i, j, k, src, planes);
 }
 
 // One thread per cell of plane q inside box b: reads E^{n+1}, H^{n+1/2} of the
@@ -180,6 +191,26 @@ cudaError_t launch_shell_E_region(const YeeArgs<T> &a, const ShellBox &o, const 
     count_launches(1);
     return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t launch_shell_E_boxes(const YeeArgs<T> &a, const BoxPlan &bp, const SourceList &src,
+                                 const PlaneList &pl, cudaStream_t st) {
+    const unsigned nb = plan_blocks(bp);
+    if (nb == 0) return cudaSuccess;
+    if (a.lossy)
+        k_shell_E_boxes<T, true><<<nb, SHELL_THREADS, 0, st>>>(a, bp, src, pl);
+    else
+        k_shell_E_boxes<T, false><<<nb, SHELL_THREADS, 0, st>>>(a, bp, src, pl);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_shell_E_boxes<float>(const YeeArgs<float> &, const BoxPlan &,
+                                                 const SourceList &, const PlaneList &,
+                                                 cudaStream_t);
+template cudaError_t launch_shell_E_boxes<double>(const YeeArgs<double> &, const BoxPlan &,
+                                                  const SourceList &, const PlaneList &,
+                                                  cudaStream_t);
 
 template <typename T>
 cudaError_t launch_shell_E(const YeeArgs<T> &a, const ShellBox &b, const SourceList &src,

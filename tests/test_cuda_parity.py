@@ -456,6 +456,41 @@ def test_fused_kernel_shapes_vs_oracle(cuda, shape, npml, lossy, dtype):
         assert np.array_equal(mg.dft(c), mo.dft[c])
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape,npml,lossy", [((48, 40, 44), 4, False), ((40, 52, 48), 8, True),
+                                              ((56, 44, 64), 12, False), ((66, 70, 72), 20, False),
+                                              ((44, 40, 40), 16, True)])
+def test_cpml_face_kernels_vs_oracle(cuda, shape, npml, lossy, dtype):
+    """Shell E through the CPML face marches (npml a multiple of 16 bytes of
+    elements): z tiles masked (npml 4, 12) or two per face (npml 20), the x-rim
+    plane and z-rim column, sources and plane DFTs inside the CPML faces, lossy
+    coefficients."""
+    g, o = both(cuda, shape, 1e-3, npml, dtype=dtype)
+    rng = np.random.default_rng(5)
+    eps = rng.uniform(1, 6, shape).astype(np.float32)
+    sig = rng.uniform(0, 50, shape) if lossy else None
+    nx, ny, nz = shape
+    for s in (g, o):
+        s.set_epsilon(eps, sigma_array=sig)
+        # a full-plane sheet crossing the x and y faces, one inside the low z face
+        s.add_source(lambda f: f.add_source_Jx(nz // 2, gaussian_sine(f.t, 40e9, 30e9),
+                                               i0=0, i1=nx, j0=0, j1=ny, rim_taper=True))
+        s.add_source(lambda f: f.add_source_Jx(1, 0.3 * gaussian_sine(f.t, 30e9, 30e9),
+                                               i0=npml + 2, i1=nx - npml - 2, j0=npml + 3,
+                                               j1=ny - npml - 1))
+    planes = [("x", 2, ("Ey", "Hz")), ("y", ny - 3, ("Ex", "Hx")), ("z", 1, ("Ez", "Hy")),
+              ("x", npml, ("Ex", "Ez"))]
+    mg = [cuda.CUDAPlaneDFTMonitor(g, ax, i, [30e9, 35e9], c) for ax, i, c in planes]
+    mo = [D.OraclePlaneDFTMonitor(o, ax, i, [30e9, 35e9], c) for ax, i, c in planes]
+    g.run(30)
+    o.run(30)
+    assert g._fused_enabled
+    assert_same(g, o)
+    for (ax, i, comps), a, b in zip(planes, mg, mo):
+        for c in comps:
+            assert np.array_equal(a.dft(c), b.dft[c]), (ax, i, c)
+
+
 def test_device_status_clean(cuda):
     import ctypes
 
@@ -494,12 +529,13 @@ def test_device_set_epsilon_equals_host_math(cuda, dtype, src_dtype, lossy):
             assert np.array_equal(co["ce"][a].cpu().numpy(), ce[a])
 
 
-def test_launch_counter_and_step_profile(cuda):
+@pytest.mark.parametrize("npml,per_step", [(6, 4), (8, 5)])
+def test_launch_counter_and_step_profile(cuda, npml, per_step):
     import ctypes
 
     from opencl_fdtd_solver_b200 import _capi as capi
 
-    g = cuda.CUDAFDTD((40, 36, 48), 1e-3, npml=6)
+    g = cuda.CUDAFDTD((40, 36, 48), 1e-3, npml=npml)
     cuda.CUDAPlaneDFTMonitor(g, 2, 20, [30e9])
     g.run(2)
     g.synchronize()
@@ -512,9 +548,11 @@ def test_launch_counter_and_step_profile(cuda):
     capi.run("fdtd_profile_read", ms, ctypes.byref(n))
     assert n.value == 5
     assert ms[0] > 0 and ms[2] > 0 and ms[3] > 0 and ms[4] > 0
-    # shell H, interior, plane DFT of the interior, shell E per step (the outer
-    # shell E slot records no launch unless the split schedule is selected)
-    assert capi.lib().fdtd_launch_count() - n0 == 4 * 5
+    # shell H, interior, then either the plane DFT of the interior and one
+    # per-cell shell E launch (npml 6), or the face marches, the per-cell
+    # kernel for the edges and rims and the plane DFT (npml 8, a multiple of
+    # four FP32 cells)
+    assert capi.lib().fdtd_launch_count() - n0 == per_step * 5
 
 
 @pytest.mark.parametrize("steps", [200, 2000], ids=["200_steps", "full_2000_steps"])
