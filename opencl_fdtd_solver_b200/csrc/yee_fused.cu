@@ -1,24 +1,27 @@
 // Fused Yee step for sm_100a: one pass over HBM for the interior of the grid.
 //
-// Schedule of fdtd_step (five launches on two streams):
+// Schedule of fdtd_step (two streams):
 //   side stream, forked from the caller's stream:
 //   1. k_shell_H   (yee_shell.cu): H^{n+1/2} on the CPML shell outside the box
 //                  B = [npml, N-npml)^3, psi_H in place, into H_next.
-//   2. k_shell_E   (yee_shell.cu): E^{n+1} of the cells outside R = [npml,
-//                  N-npml+1)^3, whose stencils read H only outside B, with the
-//                  injections and plane DFTs of those cells.
 //   caller's stream, concurrently:
-//   3. k_interior  (this file): H^{n+1/2} on B and E^{n+1} on B' = [npml+1,
+//   2. k_interior  (this file): H^{n+1/2} on B and E^{n+1} on B' = [npml+1,
 //                  N-npml)^3, into H_next / E_next, sheet injections of those
-//                  cells in the E epilogue.  Every H value its E
-//                  stencil needs lies in B and is recomputed here, so it never
-//                  waits for the shell.
-//   then, after joining the side stream:
-//   4. k_plane_dft_box (yee_shell.cu, only with plane DFT monitors): the DFTs of
-//                  the monitored planes' cells inside B', read back from the
-//                  values just written (one plane, not a field pass).
-//   5. k_shell_E   (yee_shell.cu): E^{n+1} of the one-cell rim R \ B', whose
-//                  stencils read H of B, with its injections and plane DFTs.
+//                  cells in the E epilogue.  Every H value its E stencil needs
+//                  lies in B and is recomputed here, so it never waits for the
+//                  shell.
+//   then, after joining the side stream, E^{n+1} of every cell outside B':
+//   3. k_face_E    (yee_face.cu, when npml is a multiple of 16 bytes of
+//                  elements): the six CPML face slabs as TMA plane marches,
+//                  with k_shell_E_boxes (yee_shell.cu) for the edges, corners
+//                  and a rim row on the side stream beside it;
+//   4. k_plane_dft_box (yee_shell.cu, only with plane DFT monitors): the DFTs
+//                  of the monitored planes, read back from the values just
+//                  written (one plane, not a field pass).
+//   Otherwise 3 is k_plane_dft_box over B' and 4 is k_shell_E (yee_shell.cu),
+//   one thread per shell cell with the DFTs of its cells fused.
+//   FDTD_B200_SHELL_SPLIT=1 moves the shell E cells whose stencils read no H
+//   of B onto the side stream behind k_shell_H (measured slower).
 //
 // Interior kernel.  Each CTA owns a (TJ x TK) tile of (j, k) and marches along
 // i over a chunk of planes.  Plane p is brought into shared memory by TMA
