@@ -61,50 +61,63 @@ __global__ void k_dft_faces(int nx, int ny, int nz, const T *Ex, const T *Ey, co
     if (s >= b.n_face) return;
     const FaceCoord c = face_coord(b, s);
     const int i = c.i, j = c.j, k = c.k;
+    // the face's four tangential components (Ex..Hz numbering): x faces Ey, Ez,
+    // Hy, Hz; y faces Ex, Ez, Hx, Hz; z faces Ex, Ey, Hx, Hy
+    const int g = c.face >> 1;
+    const int c0 = g == 0 ? 1 : 0, c1 = g == 2 ? 1 : 2, c2 = g == 0 ? 4 : 3, c3 = g == 2 ? 4 : 5;
+    // one frequency per thread (blockIdx.y); the four accumulator loads are
+    // issued first, before the field gathers, so they overlap one another and
+    // the gathers instead of each waiting behind the previous store
+    const int f = blockIdx.y;
+    double2 *A = reinterpret_cast<double2 *>(acc);
+    double2 *a0 = A + ((int64_t)c0 * b.nfreq + f) * b.n_face + s;
+    double2 *a1 = A + ((int64_t)c1 * b.nfreq + f) * b.n_face + s;
+    double2 *a2 = A + ((int64_t)c2 * b.nfreq + f) * b.n_face + s;
+    double2 *a3 = A + ((int64_t)c3 * b.nfreq + f) * b.n_face + s;
+    double2 q0 = *a0, q1 = *a1, q2 = *a2, q3 = *a3;
     auto at = [&](const T *F, int ii, int jj, int kk) {
         return F[((int64_t)ii * ny + jj) * nz + kk];
     };
     const T half = T(0.5), quarter = T(0.25);
-    T v[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    T t0, t1, t2, t3;  // the tangential values in the order c0..c3
     if (c.face <= 1) {
         const int k1 = (k + 1 < nz) ? k + 1 : k, j1 = (j + 1 < ny) ? j + 1 : j;
         const int ilo = (i > 0) ? i - 1 : i;
-        v[1] = (k1 != k) ? half * (at(Ey, i, j, k) + at(Ey, i, j, k1)) : at(Ey, i, j, k);
-        v[2] = (j1 != j) ? half * (at(Ez, i, j, k) + at(Ez, i, j1, k)) : at(Ez, i, j, k);
-        v[4] = quarter * (at(Hy, i, j, k) + at(Hy, ilo, j, k) + at(Hy, i, j1, k) + at(Hy, ilo, j1, k));
-        v[5] = quarter * (at(Hz, i, j, k) + at(Hz, ilo, j, k) + at(Hz, i, j, k1) + at(Hz, ilo, j, k1));
+        t0 = (k1 != k) ? half * (at(Ey, i, j, k) + at(Ey, i, j, k1)) : at(Ey, i, j, k);
+        t1 = (j1 != j) ? half * (at(Ez, i, j, k) + at(Ez, i, j1, k)) : at(Ez, i, j, k);
+        t2 = quarter * (at(Hy, i, j, k) + at(Hy, ilo, j, k) + at(Hy, i, j1, k) + at(Hy, ilo, j1, k));
+        t3 = quarter * (at(Hz, i, j, k) + at(Hz, ilo, j, k) + at(Hz, i, j, k1) + at(Hz, ilo, j, k1));
     } else if (c.face <= 3) {
         const int i1 = (i + 1 < nx) ? i + 1 : i, k1 = (k + 1 < nz) ? k + 1 : k;
         const int jlo = (j > 0) ? j - 1 : j;
-        v[0] = (k1 != k) ? half * (at(Ex, i, j, k) + at(Ex, i, j, k1)) : at(Ex, i, j, k);
-        v[2] = (i1 != i) ? half * (at(Ez, i, j, k) + at(Ez, i1, j, k)) : at(Ez, i, j, k);
-        v[3] = quarter * (at(Hx, i, j, k) + at(Hx, i, jlo, k) + at(Hx, i1, j, k) + at(Hx, i1, jlo, k));
-        v[5] = quarter * (at(Hz, i, j, k) + at(Hz, i, jlo, k) + at(Hz, i, j, k1) + at(Hz, i, jlo, k1));
+        t0 = (k1 != k) ? half * (at(Ex, i, j, k) + at(Ex, i, j, k1)) : at(Ex, i, j, k);
+        t1 = (i1 != i) ? half * (at(Ez, i, j, k) + at(Ez, i1, j, k)) : at(Ez, i, j, k);
+        t2 = quarter * (at(Hx, i, j, k) + at(Hx, i, jlo, k) + at(Hx, i1, j, k) + at(Hx, i1, jlo, k));
+        t3 = quarter * (at(Hz, i, j, k) + at(Hz, i, jlo, k) + at(Hz, i, j, k1) + at(Hz, i, jlo, k1));
     } else {
         const int i1 = (i + 1 < nx) ? i + 1 : i, j1 = (j + 1 < ny) ? j + 1 : j;
         const int klo = (k > 0) ? k - 1 : k;
-        v[0] = (j1 != j) ? half * (at(Ex, i, j, k) + at(Ex, i, j1, k)) : at(Ex, i, j, k);
-        v[1] = (i1 != i) ? half * (at(Ey, i, j, k) + at(Ey, i1, j, k)) : at(Ey, i, j, k);
-        v[3] = quarter * (at(Hx, i, j, k) + at(Hx, i, j, klo) + at(Hx, i, j1, k) + at(Hx, i, j1, klo));
-        v[4] = quarter * (at(Hy, i, j, k) + at(Hy, i, j, klo) + at(Hy, i1, j, k) + at(Hy, i1, j, klo));
+        t0 = (j1 != j) ? half * (at(Ex, i, j, k) + at(Ex, i, j1, k)) : at(Ex, i, j, k);
+        t1 = (i1 != i) ? half * (at(Ey, i, j, k) + at(Ey, i1, j, k)) : at(Ey, i, j, k);
+        t2 = quarter * (at(Hx, i, j, k) + at(Hx, i, j, klo) + at(Hx, i, j1, k) + at(Hx, i, j1, klo));
+        t3 = quarter * (at(Hy, i, j, k) + at(Hy, i, j, klo) + at(Hy, i1, j, k) + at(Hy, i1, j, klo));
     }
-    // one frequency per thread (blockIdx.y): the gathers above repeat per
-    // frequency from L1/L2, and the accumulator updates of a warp are coalesced
-    const int tang_mask = (c.face <= 1) ? 0x36 : (c.face <= 3) ? 0x2D : 0x1B;
-    double2 *A = reinterpret_cast<double2 *>(acc);
-    const int f = blockIdx.y;
-#pragma unroll
-    for (int comp = 0; comp < 6; ++comp) {
-        if (!(tang_mask & (1 << comp))) continue;
-        const double val = (double)v[comp];
-        const int h = comp >= 3 ? 2 : 0;
-        const double pr = phase[4 * f + h], pi = phase[4 * f + h + 1];
-        double2 *a = A + ((int64_t)comp * b.nfreq + f) * b.n_face + s;
-        double2 cur = *a;
-        cur.x = cur.x + val * pr;
-        cur.y = cur.y + val * pi;
-        *a = cur;
-    }
+    // E samples take the E phase of the step, H samples the H phase
+    const double epr = phase[4 * f], epi = phase[4 * f + 1];
+    const double hpr = phase[4 * f + 2], hpi = phase[4 * f + 3];
+    const double v0 = (double)t0, v1 = (double)t1, v2 = (double)t2, v3 = (double)t3;
+    q0.x = q0.x + v0 * epr;
+    q0.y = q0.y + v0 * epi;
+    q1.x = q1.x + v1 * epr;
+    q1.y = q1.y + v1 * epi;
+    q2.x = q2.x + v2 * hpr;
+    q2.y = q2.y + v2 * hpi;
+    q3.x = q3.x + v3 * hpr;
+    q3.y = q3.y + v3 * hpi;
+    *a0 = q0;
+    *a1 = q1;
+    *a2 = q2;
+    *a3 = q3;
 }
 
 constexpr int REL_THREADS = 256;
