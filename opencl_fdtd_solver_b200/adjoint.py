@@ -241,8 +241,13 @@ class EpsilonAdjoint:
                 cap0 = self._cap_all.data_ptr()
                 slot = self._cap_all[0].numel() * self._cap_all.element_size()
 
+                eptrs = {}  # E pointer arrays by buffer parity (the step ping-pongs E)
+
                 def grab(m):
-                    Ep = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in fd._E])
+                    Ep = eptrs.get(fd._parity)
+                    if Ep is None:
+                        Ep = eptrs[fd._parity] = (ctypes.c_void_p * 3)(
+                            *[t.data_ptr() for t in fd._E])
                     capi.run("fdtd_capture_box", grid, Ep, lo, hi, cap0 + m * slot, st)
 
                 grab(0)

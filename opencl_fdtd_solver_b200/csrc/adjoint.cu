@@ -300,21 +300,20 @@ __global__ void k_adj_seed(int nx, int ny, int nz, T *E0, T *E1, T *E2, AdjSeed 
     E2[idx] = ez;
 }
 
-// E over box [lo, hi) -> out[3][box cells].
+// E over box [lo, hi) -> out[3][box cells]: blockIdx.y = (component, plane),
+// threads over the plane's (j, k) cells, so the index arithmetic is one 32-bit
+// division per thread.
 template <typename T>
 __global__ void k_capture(int ny, int nz, const T *E0, const T *E1, const T *E2, int3 lo,
                           int3 ext, T *out) {
-    const int64_t nb = (int64_t)ext.x * ext.y * ext.z;
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= 3 * nb) return;
-    const int c = (int)(q / nb);
-    const int64_t r = q - c * nb;
-    const int kk = (int)(r % ext.z);
-    const int64_t t = r / ext.z;
-    const int jj = (int)(t % ext.y), ii = (int)(t / ext.y);
+    const int plane_cells = ext.y * ext.z;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= plane_cells) return;
+    const int c = blockIdx.y / ext.x, ii = blockIdx.y - c * ext.x;
+    const int jj = t / ext.z, kk = t - jj * ext.z;
     const int64_t idx = ((int64_t)(lo.x + ii) * ny + (lo.y + jj)) * nz + (lo.z + kk);
     const T *src = c == 0 ? E0 : (c == 1 ? E1 : E2);
-    out[q] = src[idx];
+    out[(int64_t)blockIdx.y * plane_cells + t] = src[idx];
 }
 
 template <typename T>
@@ -389,11 +388,12 @@ cudaError_t launch_capture(int ny, int nz, const T *const E[3], const int lo[3],
                            T *out, cudaStream_t st) {
     const int3 l = make_int3(lo[0], lo[1], lo[2]);
     const int3 ext = make_int3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
-    const int64_t n = 3 * (int64_t)ext.x * ext.y * ext.z;
-    if (n <= 0) return cudaSuccess;
+    if (ext.x <= 0 || ext.y <= 0 || ext.z <= 0) return cudaSuccess;
+    if (3 * (int64_t)ext.x > 65535 || (int64_t)ext.y * ext.z > 0x7fffffffLL)
+        return cudaErrorInvalidValue;
     const int thr = 256;
-    k_capture<T><<<(unsigned)((n + thr - 1) / thr), thr, 0, st>>>(ny, nz, E[0], E[1], E[2], l,
-                                                                 ext, out);
+    const dim3 grid((unsigned)(((int64_t)ext.y * ext.z + thr - 1) / thr), (unsigned)(3 * ext.x), 1);
+    k_capture<T><<<grid, thr, 0, st>>>(ny, nz, E[0], E[1], E[2], l, ext, out);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -405,9 +405,7 @@ cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjSeed &sd, const Ad
     bx.ntk = (hb.hi[2] - bx.k0base + L::TK - 1) / L::TK;
     const int ntj = (hb.hi[1] - bx.j0base + L::TJ - 1) / L::TJ;
     const int tiles = bx.ntk * ntj;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = device_sm_count();
     const int nplanes = hb.hi[0] - hb.lo[0];
     const int nchunk = interior_chunks(tiles, nplanes, sms);
     bx.chunk = (nplanes + nchunk - 1) / nchunk;
@@ -427,8 +425,8 @@ cudaError_t launch_adj_interior(const AdjArgs<T> &a, const AdjSeed &sd, const Ad
     }
     m.sd = sd;
     dim3 grid(tiles, (nplanes + bx.chunk - 1) / bx.chunk, 1);
-    cudaError_t e = cudaFuncSetAttribute(k_adj_interior<T, A_NSTAGE, GG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        ensure_max_dynamic_smem((const void *)k_adj_interior<T, A_NSTAGE, GG>, (int)smem);
     if (e != cudaSuccess) return e;
     k_adj_interior<T, A_NSTAGE, GG><<<grid, A_NTHREADS, smem, st>>>(maps, m, bx);
     count_launches(1);

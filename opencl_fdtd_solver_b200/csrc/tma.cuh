@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
+#include <mutex>
 
 namespace fdtd {
 
@@ -95,6 +97,43 @@ __device__ __forceinline__ void st_vec(T *p, const T (&in)[V]) {
 // the driver's encoder is unavailable or rejects the map.
 bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz, int elem,
                      int b0, int b1, int l2_promote = 256);
+
+// Host-side caches that keep the per-step launch path short (an engine calls
+// the step with the same buffers, alternating between two parities):
+//   KeyedCache : the last few values built for a key of NW 64-bit words (the
+//                tensor maps of one buffer set), one lock per lookup;
+//   device_sm_count : the SM count of the current device, queried once;
+//   ensure_max_dynamic_smem : cudaFuncSetAttribute(MaxDynamicSharedMemorySize)
+//                once per kernel, device and size.
+template <typename V, int NW, int NE = 4>
+class KeyedCache {
+  public:
+    bool get(const uint64_t (&key)[NW], V &out) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (int q = 0; q < n_; ++q)
+            if (memcmp(keys_[q], key, sizeof(key)) == 0) {
+                out = vals_[q];
+                return true;
+            }
+        return false;
+    }
+    void put(const uint64_t (&key)[NW], const V &v) {
+        std::lock_guard<std::mutex> lk(mu_);
+        const int q = n_ < NE ? n_++ : (int)(next_++ % NE);
+        memcpy(keys_[q], key, sizeof(key));
+        vals_[q] = v;
+    }
+
+  private:
+    std::mutex mu_;
+    uint64_t keys_[NE][NW];
+    V vals_[NE];
+    int n_ = 0;
+    unsigned next_ = 0;
+};
+
+int device_sm_count();
+cudaError_t ensure_max_dynamic_smem(const void *func, int bytes);
 
 // A stream of this host thread and device, with events to fork from and join
 // back to a caller's stream.  slot 0 serves the forward step, slot 1 the

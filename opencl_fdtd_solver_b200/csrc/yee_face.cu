@@ -440,8 +440,8 @@ template <typename T, bool LOSSY, int NSTAGE, int AXS>
 cudaError_t launch_face_kernel(const FaceMaps &maps, const YeeArgs<T> &a, const FaceSet &fs,
                                const SourceList &src, int ctas, size_t smem, cudaStream_t st) {
     if (ctas <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_face_E<T, LOSSY, NSTAGE, AXS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        ensure_max_dynamic_smem((const void *)k_face_E<T, LOSSY, NSTAGE, AXS>, (int)smem);
     if (e != cudaSuccess) return e;
     k_face_E<T, LOSSY, NSTAGE, AXS><<<ctas, FACE_THREADS, smem, st>>>(maps, a, fs, src);
     count_launches(1);
@@ -469,6 +469,24 @@ bool build_face_maps(const YeeArgs<T> &a, FaceMaps &m) {
     using L0 = FaceTile<T, 0>;
     using L2 = FaceTile<T, 2>;
     const int elem = (int)sizeof(T), nx = a.nx, ny = a.ny, nz = a.nz, p2 = 2 * a.npml;
+    // the maps of this buffer set, built once
+    static KeyedCache<FaceMaps, 20> cache;
+    uint64_t key[20];
+    for (int c = 0; c < 3; ++c) {
+        key[c] = (uint64_t)(uintptr_t)a.E[c];
+        key[3 + c] = (uint64_t)(uintptr_t)a.H_next[c];
+        key[6 + c] = (uint64_t)(uintptr_t)a.ce[c];
+        key[9 + c] = a.lossy ? (uint64_t)(uintptr_t)a.ca[c] : 0;
+    }
+    key[12] = (uint64_t)(uintptr_t)a.psi_e[0];
+    key[13] = (uint64_t)(uintptr_t)a.psi_e[1];
+    key[14] = (uint64_t)(uintptr_t)a.psi_e[2];
+    key[15] = (uint64_t)(uintptr_t)a.psi_e[3];
+    key[16] = (uint64_t)(uintptr_t)a.psi_e[4];
+    key[17] = (uint64_t)(uintptr_t)a.psi_e[5];
+    key[18] = ((uint64_t)nx << 40) ^ ((uint64_t)ny << 20) ^ (uint64_t)nz;
+    key[19] = ((uint64_t)a.npml << 1) | (uint64_t)(a.lossy != 0);
+    if (cache.get(key, m)) return true;
     memset(&m, 0, sizeof(m));
     const int hw[2] = {L0::HW, L2::HW}, hh[2] = {L0::HH, L2::HH};
     const int tk[2] = {L0::TK, L2::TK}, tj[2] = {L0::TJ, L2::TJ};
@@ -489,12 +507,15 @@ bool build_face_maps(const YeeArgs<T> &a, FaceMaps &m) {
                 return false;
         }
     // ψ stripes: x (2P, ny, nz), y (nx, 2P, nz), z (nx, ny, 2P)
-    return make_tensor_map(&m.P[0][0], a.psi_e[2], p2, ny, nz, elem, L0::TK, L0::TJ) &&
-           make_tensor_map(&m.P[0][1], a.psi_e[4], p2, ny, nz, elem, L0::TK, L0::TJ) &&
-           make_tensor_map(&m.P[1][0], a.psi_e[0], nx, p2, nz, elem, L0::TK, L0::TJ) &&
-           make_tensor_map(&m.P[1][1], a.psi_e[5], nx, p2, nz, elem, L0::TK, L0::TJ) &&
-           make_tensor_map(&m.P[2][0], a.psi_e[1], nx, ny, p2, elem, L2::TK, L2::TJ, 0) &&
-           make_tensor_map(&m.P[2][1], a.psi_e[3], nx, ny, p2, elem, L2::TK, L2::TJ, 0);
+    const bool ok =
+        make_tensor_map(&m.P[0][0], a.psi_e[2], p2, ny, nz, elem, L0::TK, L0::TJ) &&
+        make_tensor_map(&m.P[0][1], a.psi_e[4], p2, ny, nz, elem, L0::TK, L0::TJ) &&
+        make_tensor_map(&m.P[1][0], a.psi_e[0], nx, p2, nz, elem, L0::TK, L0::TJ) &&
+        make_tensor_map(&m.P[1][1], a.psi_e[5], nx, p2, nz, elem, L0::TK, L0::TJ) &&
+        make_tensor_map(&m.P[2][0], a.psi_e[1], nx, ny, p2, elem, L2::TK, L2::TJ, 0) &&
+        make_tensor_map(&m.P[2][1], a.psi_e[3], nx, ny, p2, elem, L2::TK, L2::TJ, 0);
+    if (ok) cache.put(key, m);
+    return ok;
 }
 
 void set_region(FaceBox &f, int r, const int lo[3], const int hi[3]) {

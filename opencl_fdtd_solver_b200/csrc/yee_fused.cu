@@ -536,6 +536,20 @@ template <typename T, int GG>
 bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
     using L = Tile<T, GG>;
     const int elem = (int)sizeof(T);
+    // the maps of this buffer set, built once
+    static KeyedCache<FusedMaps, 16> cache;
+    uint64_t key[16];
+    for (int c = 0; c < 3; ++c) {
+        key[c] = (uint64_t)(uintptr_t)a.E[c];
+        key[3 + c] = (uint64_t)(uintptr_t)a.H[c];
+        key[6 + c] = (uint64_t)(uintptr_t)a.ce[c];
+        key[9 + c] = a.lossy ? (uint64_t)(uintptr_t)a.ca[c] : 0;
+    }
+    key[12] = (uint64_t)a.nx;
+    key[13] = (uint64_t)a.ny;
+    key[14] = (uint64_t)a.nz;
+    key[15] = (uint64_t)(a.lossy != 0);
+    if (cache.get(key, maps)) return true;
     memset(&maps, 0, sizeof(maps));
     for (int c = 0; c < 3; ++c) {
         if (!make_tensor_map(&maps.E[c], a.E[c], a.nx, a.ny, a.nz, elem, L::EW, L::EH) ||
@@ -545,6 +559,7 @@ bool build_maps(const YeeArgs<T> &a, FusedMaps &maps) {
         if (a.lossy && !make_tensor_map(&maps.A[c], a.ca[c], a.nx, a.ny, a.nz, elem, L::TK, L::TJ))
             return false;
     }
+    cache.put(key, maps);
     return true;
 }
 
@@ -562,9 +577,7 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
     bx.ntk = (hb.hi[2] - bx.k0base + L::TK - 1) / L::TK;
     const int ntj = (hb.hi[1] - bx.j0base + L::TJ - 1) / L::TJ;
     const int tiles = bx.ntk * ntj;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = device_sm_count();
     const int nplanes = hb.hi[0] - hb.lo[0];
     const int nchunk = choose_chunks(tiles, nplanes, sms);
     bx.chunk = (nplanes + nchunk - 1) / nchunk;
@@ -578,8 +591,7 @@ cudaError_t launch_interior(const YeeArgs<T> &a, const FusedMaps &maps, const Sh
     cudaError_t e = cudaSuccess;
 #define FDTD_LAUNCH_INTERIOR(LS, NS)                                                           \
     do {                                                                                       \
-        e = cudaFuncSetAttribute(k_interior<T, LS, NS, GG>,                                    \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+        e = ensure_max_dynamic_smem((const void *)k_interior<T, LS, NS, GG>, (int)smem);       \
         if (e != cudaSuccess) return e;                                                        \
         k_interior<T, LS, NS, GG><<<grid, NTHREADS, smem, st>>>(maps, a, bx, src);             \
         count_launches(1);                                                                     \
@@ -664,6 +676,40 @@ void prof_end(const std::array<cudaEvent_t, NEV> &ev, bool dft_last) {
 // Joined back to the caller's stream by an event before the rim E cells.
 namespace {
 thread_local std::unordered_map<int, SideStream> t_side;
+}
+
+int device_sm_count() {
+    static std::atomic<int> sms[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int v = sms[dev].load();
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            v <= 0)
+            return 148;
+        sms[dev].store(v);
+    }
+    return v;
+}
+
+cudaError_t ensure_max_dynamic_smem(const void *func, int bytes) {
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, int> set;  // (function, device) -> bytes set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t key = (uint64_t)(uintptr_t)func * 64u + (uint64_t)(dev & 63);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = set.find(key);
+        if (it != set.end() && it->second >= bytes) return cudaSuccess;
+    }
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int &v = set[key];
+    if (bytes > v) v = bytes;
+    return cudaSuccess;
 }
 
 cudaError_t side_stream(SideStream **out, int slot) {
