@@ -997,30 +997,40 @@ def run_huygens_leg(args):
     """Cost of the Huygens-box face DFT (89³ box, 8 frequencies) on the medium
     configuration: ms per step with and without the box monitor, device time by
     CUDA events on the engine's stream and host wall time (the monitor's launch
-    is issued from its Python callback after each step).  The reference quotes
-    about 1.5 % for its fused 6-face DFT (README.md:192)."""
+    is issued from its Python callback after each step).  The two engines run
+    alternately, three windows each, and the medians are compared, so that a
+    drift of the board's clock between windows does not enter the difference.
+    The reference quotes about 1.5 % for its fused 6-face DFT (README.md:192)."""
     import torch
 
     k = args.huygens_steps
     out = {"workload": f"medium_{MED_N}^3_fp32_npml{MED_NPML}_sphere_sheet_box"
-                       f"{2 * MED_HALF + 1}^3_{MED_FREQS.size}freqs", "steps": k}
-    for tag, box in (("no_box", False), ("box", True)):
-        g, mon = medium_engine(box=box)
+                       f"{2 * MED_HALF + 1}^3_{MED_FREQS.size}freqs", "steps_per_window": k,
+           "windows": 3}
+    engines = {tag: medium_engine(box=box) for tag, box in (("no_box", False), ("box", True))}
+    for g, _ in engines.values():
         for _ in range(args.warmup):
             g.step()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
-        e0.record(g.queue)
-        for _ in range(k):
-            g.step()
-        e1.record(g.queue)
-        torch.cuda.synchronize()
-        out[f"{tag}_wall_ms_per_step"] = round((time.perf_counter() - t0) / k * 1e3, 4)
-        out[f"{tag}_device_ms_per_step"] = round(e0.elapsed_time(e1) / k, 4)
-        del g, mon
-        torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    times = {tag: {"wall": [], "device": []} for tag in engines}
+    for _ in range(3):
+        for tag, (g, _) in engines.items():
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e0.record(g.queue)
+            for _ in range(k):
+                g.step()
+            e1.record(g.queue)
+            torch.cuda.synchronize()
+            times[tag]["wall"].append((time.perf_counter() - t0) / k * 1e3)
+            times[tag]["device"].append(e0.elapsed_time(e1) / k)
+    for tag in engines:
+        for kind in ("wall", "device"):
+            out[f"{tag}_{kind}_ms_per_step"] = round(float(np.median(times[tag][kind])), 4)
+    del engines
+    torch.cuda.empty_cache()
     for kind in ("wall", "device"):
         a, b = out[f"no_box_{kind}_ms_per_step"], out[f"box_{kind}_ms_per_step"]
         out[f"overhead_{kind}_pct"] = round(100.0 * (b - a) / a, 2)

@@ -383,8 +383,9 @@ const char *fdtd_last_error(void);
 int fdtd_device_status(int32_t *flags, int32_t reset);
 
 /* Budget of the bounded pipeline waits of one kernel, for later launches from
- * this process: kernel FDTD_WAIT_INTERIOR (the fused step's interior kernel;
- * budget in mbarrier polls, default and maximum 2^24) or FDTD_WAIT_N2F (the
+ * this process: kernel FDTD_WAIT_INTERIOR (the fused step's interior kernel,
+ * its CPML face marches and the adjoint interior march; budget in mbarrier
+ * polls, default and maximum 2^24) or FDTD_WAIT_N2F (the
  * tensor-core near-to-far contraction; budget in nanoseconds, default 2e8).
  * budget < 0 restores the default; 0 makes a wait give up unless its phase has
  * already completed, which exercises the timeout path: the kernel raises its

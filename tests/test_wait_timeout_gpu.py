@@ -1,7 +1,7 @@
 """The bounded device waits give up, report and recover (GPU).
 
-The fused step's interior kernel and the tensor-core near-to-far contraction
-wait on mbarriers for their bulk copies and MMAs.  Each wait has a budget, and
+The fused step's interior kernel and CPML face marches and the tensor-core
+near-to-far contraction wait on mbarriers for their bulk copies and MMAs.  Each wait has a budget, and
 ``fdtd_set_wait_budget`` lowers it for later launches.  With a budget of zero a
 wait gives up unless its phase is already complete, which is certain for the
 first plane of the interior march and for the contraction's first accumulator
@@ -48,11 +48,11 @@ def _status(capi, reset):
     return flags.value
 
 
-def _engines():
+def _engines(npml=6):
     from opencl_fdtd_solver_b200 import CUDAFDTD
     from oracle.cpu_fdtd import OracleFDTD
 
-    shape, npml = (40, 36, 48), 6
+    shape = (40, 36, 48)
     g = CUDAFDTD(shape, 1e-3, npml=npml)
     o = OracleFDTD(shape, 1e-3, npml=npml)
 
@@ -64,9 +64,12 @@ def _engines():
     return g, o
 
 
-def test_interior_wait_timeout_reports_and_recovers(capi):
+@pytest.mark.parametrize("npml", [6, 8])
+def test_interior_wait_timeout_reports_and_recovers(capi, npml):
+    """npml 6: the interior march gives up; npml 8 (a multiple of four FP32
+    cells): the CPML face marches of the shell E step give up as well."""
     assert capi.call("fdtd_set_wait_budget", 7, 0) == capi.FDTD_ERR_INVALID
-    g, _ = _engines()
+    g, _ = _engines(npml)
     g.run(3)
     assert g._fused_enabled
     capi.run("fdtd_set_wait_budget", capi.FDTD_WAIT_INTERIOR, 0)
@@ -77,7 +80,7 @@ def test_interior_wait_timeout_reports_and_recovers(capi):
     assert _status(capi, 0) == 0
     capi.run("fdtd_set_wait_budget", capi.FDTD_WAIT_INTERIOR, -1)
     # a fresh engine with the default budget matches the oracle bit for bit
-    g, o = _engines()
+    g, o = _engines(npml)
     g.run(30)
     o.run(30)
     assert _status(capi, 0) == 0
