@@ -130,9 +130,11 @@ int fdtd_update_E(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
 /* One full leapfrog step H -> sources -> E: reads E/H, writes E_next/H_next,
  * ψ stripes in place.  The interior box [npml, N-npml)^3 is updated by one
  * single-pass kernel (H and E per plane, one read and one write of each array);
- * the CPML shell around it by per-cell kernels: its H on a library-owned side
+ * the CPML shell around it: its H by a per-cell kernel on a library-owned side
  * stream (per host thread and device) that overlaps the interior kernel and is
- * joined back by an event, its E afterwards on the caller's stream.
+ * joined back by an event, its E afterwards on the caller's stream, as plane
+ * marches over the six CPML face slabs (when npml is a multiple of 16 bytes of
+ * elements) with the edges and rims per cell on the side stream, or per cell.
  * Replaces the whole of OpenCLFDTD.step() up to the monitors
  * (engine.py:724-735): _update_H, the source callbacks' injections, _update_E. */
 int fdtd_step(const fdtd_grid *g, const fdtd_fields *f, const fdtd_cpml *c,
@@ -364,8 +366,10 @@ int fdtd_set_epsilon(const fdtd_grid *g, const void *eps, const void *sigma, int
  * launch, [0] CPML-shell H on the side stream (concurrent with [2]), [1] the
  * shell E cells run on the side stream (none unless FDTD_B200_SHELL_SPLIT=1
  * selects that schedule), [2] the interior single-pass kernel, [3] the plane
- * DFT of the interior, [4] the shell E cells after the join (with sources and
- * DFTs), and the number of steps recorded.  No reference counterpart. */
+ * DFT (of the interior cells, or with the face marches of the whole planes),
+ * [4] the shell E cells after the join (the face marches and the per-cell
+ * edges beside them, or the per-cell kernel with sources and DFTs), and the
+ * number of steps recorded.  No reference counterpart. */
 int fdtd_profile_steps(int32_t enable);
 int fdtd_profile_read(double ms[5], int32_t *nsteps);
 
