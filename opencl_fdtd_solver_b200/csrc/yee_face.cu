@@ -548,8 +548,8 @@ bool faces_enabled() {
 // (P = npml, I = [P+1, N-P)): the x edges of the planes [0, P] and [N-P, N)
 // (j or k in a CPML slab), the four y-z corner blocks of the I planes and the
 // rim row j = P of the I planes.
-void face_partition(int nx, int ny, int nz, int P, int out_lo[6][3], int out_hi[6][3],
-                    BoxPlan &rest) {
+static void face_partition(int nx, int ny, int nz, int P, int out_lo[6][3], int out_hi[6][3],
+                           BoxPlan &rest) {
     const int reg[6][6] = {
         {0, P + 1, P, ny - P, P, nz - P},          {nx - P, nx, P, ny - P, P, nz - P},
         {P + 1, nx - P, 0, P, P, nz - P},          {P + 1, nx - P, ny - P, ny, P, nz - P},
@@ -601,7 +601,8 @@ cudaError_t launch_shell_E_faces(const YeeArgs<T> &a, const SourceList &src, cud
     using L0 = FaceTile<T, 0>;
     using L2 = FaceTile<T, 2>;
     FaceMaps maps;
-    if (!build_face_maps<T>(a, maps)) return cudaErrorInvalidValue;
+    // nothing launched yet: the caller takes the per-cell shell E instead
+    if (!build_face_maps<T>(a, maps)) return cudaErrorNotSupported;
     int lo[6][3], hi[6][3];
     BoxPlan rest;
     face_partition(a.nx, a.ny, a.nz, a.npml, lo, hi, rest);

@@ -857,11 +857,17 @@ cudaError_t launch_step_fused(const YeeArgs<T> &a, const SourceList &src, const 
         }
     }
     if (prof) cudaEventRecord(ev[4], st);
-    const bool faces = use_interior && !split_shell_e() && face_path_ok<T>(a);
-    if (faces) {
+    bool faces = use_interior && !split_shell_e() && face_path_ok<T>(a);
+    if (faces && e == cudaSuccess) {
         // shell E through the CPML face marches, then the plane DFTs of every
         // monitored cell in one pass over the planes
-        if (e == cudaSuccess) e = launch_shell_E_faces<T>(a, src, st, side);
+        e = launch_shell_E_faces<T>(a, src, st, side);
+        if (e == cudaErrorNotSupported) {
+            faces = false;  // no tensor maps: the per-cell shell E below
+            e = cudaSuccess;
+        }
+    }
+    if (faces) {
         if (prof) cudaEventRecord(ev[5], st);
         if (e == cudaSuccess && pl.n) e = launch_plane_dft_box<T>(a, all, pl, st);
     } else {

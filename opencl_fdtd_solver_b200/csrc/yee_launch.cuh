@@ -53,9 +53,10 @@ struct SideStream;
 // Shell E of the fused step through the CPML face kernels (yee_face.cu): the
 // six face slabs as TMA plane marches on st, the remaining shell cells by the
 // per-cell kernel on the side stream, joined back to st; no plane DFTs (the
-// caller accumulates the monitored planes afterwards).  face_path_ok: the grid
-// qualifies (whole grid, npml a multiple of 16 bytes of elements, aligned
-// stripes).
+// caller accumulates the monitored planes afterwards); cudaErrorNotSupported,
+// with nothing launched, when the tensor maps cannot be built.  face_path_ok:
+// the grid qualifies (whole grid, npml a multiple of 16 bytes of elements,
+// aligned stripes).
 template <typename T>
 bool face_path_ok(const YeeArgs<T> &a);
 template <typename T>
