@@ -533,13 +533,20 @@ void set_chunks(FaceBox &f, int nplanes) {
     f.chunk = nplanes > 0 ? ceil_div(nplanes, f.nchunk) : 1;
 }
 
-// FDTD_B200_FACE_E=0 runs every shell E cell through the per-cell kernel.
-bool faces_enabled() {
-    static const bool v = [] {
-        const char *e = getenv("FDTD_B200_FACE_E");
-        return !(e && atoi(e) == 0);
-    }();
-    return v;
+// The face marches pay off only for a large shell: measured per step (FP32,
+// one plane DFT, interleaved runs) they were slower than the per-cell kernel at
+// 160x160x96 (86.2 against 73.7 us), 256^3 (312.6 / 311.3 us at npml 16) and
+// 384^3 (859 / 851 us), and faster at 512^3 (1.854 / 1.877 ms, 24.3 M shell E
+// cells); FP64 at 384^3 was slower too (1578.6 against 1562.2 us).
+// FDTD_B200_FACE_E (read at every step) forces them on ("1", whenever the grid
+// qualifies) or off ("0"); unset, they take shells of at least FACE_MIN_CELLS
+// E cells.
+constexpr int64_t FACE_MIN_CELLS = 20000000;
+
+int face_mode() {
+    const char *e = getenv("FDTD_B200_FACE_E");
+    if (!e || !*e) return -1;
+    return atoi(e) != 0 ? 1 : 0;
 }
 
 }  // namespace
@@ -580,10 +587,16 @@ template <typename T>
 bool face_path_ok(const YeeArgs<T> &a) {
     constexpr int V = 16 / (int)sizeof(T);
     const int P = a.npml;
-    if (!faces_enabled() || P < V || P % V != 0 || a.nz % V != 0 || P + 1 > FACE_MAX_CHUNK)
+    const int mode = face_mode();
+    if (mode == 0 || P < V || P % V != 0 || a.nz % V != 0 || P + 1 > FACE_MAX_CHUNK)
         return false;
     if (a.xb.pml_lo != P || a.xb.pml_hi != P || a.ghost_lo != 0 || a.ghost_hi != 0) return false;
     if (a.nx - 2 * P < 2 || a.ny - 2 * P < 2 || a.nz - 2 * P < 2) return false;
+    if (mode < 0) {
+        const int64_t all = (int64_t)a.nx * a.ny * a.nz;
+        const int64_t in = (int64_t)(a.nx - 2 * P - 1) * (a.ny - 2 * P - 1) * (a.nz - 2 * P - 1);
+        if (all - in < FACE_MIN_CELLS) return false;
+    }
     for (int c = 0; c < 3; ++c) {
         const void *ptrs[4] = {a.E[c], a.H_next[c], a.ce[c], a.E_next[c]};
         for (const void *q : ptrs)

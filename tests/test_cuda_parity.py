@@ -460,11 +460,13 @@ def test_fused_kernel_shapes_vs_oracle(cuda, shape, npml, lossy, dtype):
 @pytest.mark.parametrize("shape,npml,lossy", [((48, 40, 44), 4, False), ((40, 52, 48), 8, True),
                                               ((56, 44, 64), 12, False), ((66, 70, 72), 20, False),
                                               ((44, 40, 40), 16, True)])
-def test_cpml_face_kernels_vs_oracle(cuda, shape, npml, lossy, dtype):
+def test_cpml_face_kernels_vs_oracle(cuda, shape, npml, lossy, dtype, monkeypatch):
     """Shell E through the CPML face marches (npml a multiple of 16 bytes of
-    elements): z tiles masked (npml 4, 12) or two per face (npml 20), the x-rim
+    elements; forced on, since by default they take only shells of 20 M cells
+    and more): z tiles masked (npml 4, 12) or two per face (npml 20), the x-rim
     plane and z-rim column, sources and plane DFTs inside the CPML faces, lossy
     coefficients."""
+    monkeypatch.setenv("FDTD_B200_FACE_E", "1")
     g, o = both(cuda, shape, 1e-3, npml, dtype=dtype)
     rng = np.random.default_rng(5)
     eps = rng.uniform(1, 6, shape).astype(np.float32)
@@ -529,12 +531,14 @@ def test_device_set_epsilon_equals_host_math(cuda, dtype, src_dtype, lossy):
             assert np.array_equal(co["ce"][a].cpu().numpy(), ce[a])
 
 
-@pytest.mark.parametrize("npml,per_step", [(6, 4), (8, 5)])
-def test_launch_counter_and_step_profile(cuda, npml, per_step):
+@pytest.mark.parametrize("npml,faces,per_step", [(6, None, 4), (8, None, 4), (8, "1", 5)])
+def test_launch_counter_and_step_profile(cuda, npml, faces, per_step, monkeypatch):
     import ctypes
 
     from opencl_fdtd_solver_b200 import _capi as capi
 
+    if faces is not None:
+        monkeypatch.setenv("FDTD_B200_FACE_E", faces)
     g = cuda.CUDAFDTD((40, 36, 48), 1e-3, npml=npml)
     cuda.CUDAPlaneDFTMonitor(g, 2, 20, [30e9])
     g.run(2)
@@ -549,9 +553,9 @@ def test_launch_counter_and_step_profile(cuda, npml, per_step):
     assert n.value == 5
     assert ms[0] > 0 and ms[2] > 0 and ms[3] > 0 and ms[4] > 0
     # shell H, interior, then either the plane DFT of the interior and one
-    # per-cell shell E launch (npml 6), or the face marches, the per-cell
-    # kernel for the edges and rims and the plane DFT (npml 8, a multiple of
-    # four FP32 cells)
+    # per-cell shell E launch (the default for a shell this small), or the
+    # face marches, the per-cell kernel for the edges and rims and the plane
+    # DFT (forced on; npml 8 is a multiple of four FP32 cells)
     assert capi.lib().fdtd_launch_count() - n0 == per_step * 5
 
 
