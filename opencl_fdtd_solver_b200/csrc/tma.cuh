@@ -104,7 +104,7 @@ bool make_tensor_map(CUtensorMap *out, const void *base, int nx, int ny, int nz,
 //                tensor maps of one buffer set), one lock per lookup;
 //   device_sm_count : the SM count of the current device, queried once;
 //   ensure_max_dynamic_smem : cudaFuncSetAttribute(MaxDynamicSharedMemorySize)
-//                once per kernel, device and size.
+//                only when the kernel's current limit is below the size.
 template <typename V, int NW, int NE = 4>
 class KeyedCache {
   public:

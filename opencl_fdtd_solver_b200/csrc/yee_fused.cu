@@ -692,24 +692,14 @@ int device_sm_count() {
     return v;
 }
 
+// Reads the function's current limit (per context, so a device reset that
+// restores the default is seen) and raises it only when it is too low.
 cudaError_t ensure_max_dynamic_smem(const void *func, int bytes) {
-    static std::mutex mu;
-    static std::unordered_map<uint64_t, int> set;  // (function, device) -> bytes set
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, func);
     if (e != cudaSuccess) return e;
-    const uint64_t key = (uint64_t)(uintptr_t)func * 64u + (uint64_t)(dev & 63);
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        auto it = set.find(key);
-        if (it != set.end() && it->second >= bytes) return cudaSuccess;
-    }
-    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e != cudaSuccess) return e;
-    std::lock_guard<std::mutex> lk(mu);
-    int &v = set[key];
-    if (bytes > v) v = bytes;
-    return cudaSuccess;
+    if (fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t side_stream(SideStream **out, int slot) {
